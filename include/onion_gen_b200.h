@@ -1,0 +1,168 @@
+/*
+ * onion_gen_b200 — C ABI of the B200 key-search engine.
+ *
+ * A drop-in for the device engine onion-gen exposes to its run driver
+ * (src/gpu/mod.rs:292-477, backend src/gpu/cuda.rs:103-365): a chain of
+ * candidates starting at a point, filtered on the device by a prefix bitmap,
+ * returning every (offset, packed key) the bitmap did not rule out.
+ *
+ * Conventions
+ *   - Every call returns 0 (OG_OK) or an og_status; a message goes to
+ *     `err` (NUL-terminated, truncated to `errlen`) when `err` is not NULL.
+ *   - Field elements and keys are 32 little-endian bytes. A point is four
+ *     field elements X, Y, Z, T (extended coordinates), 128 bytes.
+ *   - An offset is the scalar delta of a candidate from the start point's
+ *     scalar, always a multiple of 8 (src/gpu/mod.rs:113-119).
+ *   - A packed key is the canonical y coordinate with the sign bit (bit 255)
+ *     clear (src/gpu/mod.rs:117-118).
+ *   - An engine is used by one thread at a time; distinct engines are
+ *     independent.
+ */
+#ifndef ONION_GEN_B200_H
+#define ONION_GEN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum og_status {
+    OG_OK = 0,
+    OG_E_ARG = 1,        /* an argument is out of range */
+    OG_E_NODEVICE = 2,   /* no driver or no device (src/gpu/cuda.rs:35-77) */
+    OG_E_DEVICE = 3,     /* a CUDA call failed */
+    OG_E_NOMEM = 4,      /* device or host memory could not be allocated */
+    OG_E_OVERFLOW = 5,   /* more survivors than room: never truncated (src/gpu/cuda.rs:356-362) */
+    OG_E_CAPACITY = 6,   /* the caller's output buffer is smaller than og_*_room() */
+    OG_E_FILTER = 7,     /* a filter did not parse, or no index could be built */
+    OG_E_STATE = 8,      /* call not valid in this state (unknown search, closed engine) */
+    OG_E_TIMEOUT = 9,    /* a bounded wait ran out */
+    OG_E_VERIFY = 10     /* an independent re-derivation disagreed with the device */
+};
+
+/* One candidate the bitmap did not rule out — gpu::Survivor
+ * (src/gpu/mod.rs:113-119). */
+typedef struct og_survivor {
+    uint64_t offset;
+    uint8_t packed[32];
+} og_survivor;
+
+/* ---- devices: cuda::look (src/gpu/cuda.rs:35-77) ----------------------- */
+
+/* Number of CUDA devices; OG_E_NODEVICE when there is no driver or none. */
+int og_device_count(int* count, char* err, size_t errlen);
+/* Name and total memory of device `ordinal`. */
+int og_device_info(int ordinal, char* name, size_t namelen, uint64_t* memory, int* sms, char* err,
+                   size_t errlen);
+
+/* ---- the engine: gpu::Engine (src/gpu/mod.rs:292-477) ------------------- */
+
+typedef struct og_engine og_engine;
+
+/* Replaces gpu::Engine::new(device, start, threads, bitmap, bitmap_bits,
+ * retune) (src/gpu/mod.rs:346-413) and cuda::Engine::new
+ * (src/gpu/cuda.rs:145-270). `start` is the chain's first point (s * B);
+ * `threads` is the number of lanes, 0 to take the shape from tuning.yaml
+ * or, failing that (or with `retune`), from a timed walk that is then
+ * recorded there (src/tuning.rs). `bitmap` holds `words` 64-bit words of a
+ * prefix index `bits` wide (FilterSet::index_words, src/filter.rs:1857). */
+int og_engine_new(int ordinal, const uint8_t start[128], uint32_t threads, const uint64_t* bitmap,
+                  size_t words, uint32_t bits, int retune, og_engine** out, char* err, size_t errlen);
+
+/* Enumeration schemes. */
+enum og_scheme {
+    OG_SCHEME_PAIRED = 0, /* y(P +- Q_m) around an affine centre, one inversion per round */
+    OG_SCHEME_CHAIN = 1   /* +8G chain, Z batch-inverted over n steps (src/batch.rs) */
+};
+
+/* Launch shape of an engine. Zero fields take defaults. */
+typedef struct og_engine_config {
+    uint32_t scheme;   /* og_scheme */
+    uint32_t half;     /* paired: table size; a round is 2*half+1 candidates. chain: n steps */
+    uint32_t lanes;    /* lanes (independent chains), a multiple of `block` */
+    uint32_t rounds;   /* rounds per advance */
+    uint32_t block;    /* threads per CUDA block, a multiple of 32 */
+    uint32_t dump;     /* 1: ignore the bitmap, every candidate survives (parity runs) */
+    uint32_t room;     /* survivor records per advance; 0 sizes it from the bitmap's occupancy */
+} og_engine_config;
+
+/* The same engine with an explicit shape (no tuning). `bitmap` may be NULL
+ * only with cfg->dump = 1. */
+int og_engine_new_config(int ordinal, const uint8_t start[128], const og_engine_config* cfg,
+                         const uint64_t* bitmap, size_t words, uint32_t bits, og_engine** out, char* err,
+                         size_t errlen);
+
+/* Engine::threads (src/gpu/mod.rs:452): lanes. */
+uint32_t og_engine_threads(const og_engine* e);
+/* Engine::batch (src/gpu/mod.rs:461): candidates examined per advance. */
+uint64_t og_engine_batch(const og_engine* e);
+/* Survivor records one advance can return: the size `out` must have. */
+size_t og_engine_room(const og_engine* e);
+/* The shape in use. */
+void og_engine_shape(const og_engine* e, og_engine_config* cfg);
+
+/* Engine::advance (src/gpu/mod.rs:470, src/gpu/cuda.rs:282-365): moves every
+ * lane on by one launch and writes each survivor to `out` (room `cap`),
+ * their number to `*n`. More survivors than the engine's room is
+ * OG_E_OVERFLOW, never a silent truncation. */
+int og_engine_advance(og_engine* e, og_survivor* out, size_t cap, size_t* n, char* err, size_t errlen);
+
+/* Device time of the last advance's kernel, milliseconds (CUDA events on the
+ * engine's stream). */
+float og_engine_last_kernel_ms(const og_engine* e);
+
+void og_engine_free(og_engine* e);
+
+/* ---- measurement --------------------------------------------------------- */
+
+/* The integer-multiply roofline of device `ordinal`, measured: the issue
+ * rate of independent 32-bit multiply-adds (per second) and the partial
+ * products per second that independent field multiplications achieve.
+ * No counterpart in the reference (its engine reports candidates/s only). */
+int og_measure_int_peak(int ordinal, double* imad_per_s, double* mul_pp_per_s, char* err, size_t errlen);
+
+/* ---- host side of the hit path ------------------------------------------ */
+
+/* key::secret_scalar (src/key.rs:23-29). */
+void og_secret_scalar(const uint8_t seed[32], uint8_t scalar[32]);
+/* key::expanded_secret_key (src/key.rs:33-39). */
+void og_expanded_secret_key(const uint8_t seed[32], uint8_t out[64]);
+/* key::expanded_secret_at_offset (src/key.rs:167-177): 0 when clamping broke. */
+int og_expanded_secret_at_offset(const uint8_t seed[32], uint64_t offset, uint8_t out[64]);
+/* curve::scalar_base_mult (src/curve.rs:188-198), point as X,Y,Z,T. */
+void og_scalar_base_mult(const uint8_t scalar[32], uint8_t point[128]);
+/* key::pack (src/key.rs:55-62). */
+void og_pack(const uint8_t point[128], uint8_t out[32]);
+/* key::address (src/key.rs:118-132), 56 symbols + NUL. */
+void og_address(const uint8_t pk[32], char out[57]);
+/* run::block_seed (src/run.rs:211-221). */
+void og_block_seed(const uint8_t root[32], uint64_t index, uint8_t out[32]);
+/* The device-key recheck of src/run.rs:1089-1104: re-derives the candidate
+ * at `offset` from `seed` and compares it with `packed` (sign masked).
+ * OG_OK fills the full public key and the 64-byte secret; OG_E_VERIFY on a
+ * mismatch; OG_E_ARG when the offset broke clamping. */
+int og_check_hit(const uint8_t seed[32], uint64_t offset, const uint8_t packed[32], uint8_t pk[32],
+                 uint8_t secret[64]);
+
+/* ---- prefix filters: FilterSet (src/filter.rs) ------------------------- */
+
+typedef struct og_filters og_filters;
+
+/* Newline-separated literal prefixes; bits = 0 chooses the index width. */
+int og_filters_new(const char* text, uint32_t bits, og_filters** out, char* err, size_t errlen);
+size_t og_filters_count(const og_filters* f);
+/* canonical text of kept filter i (sorted, absorbed) */
+int og_filters_text(const og_filters* f, size_t i, char* out, size_t cap);
+uint32_t og_filters_bits(const og_filters* f);
+size_t og_filters_words(const og_filters* f, const uint64_t** words);
+double og_filters_occupancy(const og_filters* f);
+/* FilterSet::match_key (src/filter.rs:2098): index of the match or -1. */
+long og_filters_match(const og_filters* f, const uint8_t packed[32]);
+void og_filters_free(og_filters* f);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,115 @@
+"""ctypes binding of libonion_gen_b200.so (the C ABI in include/onion_gen_b200.h).
+
+The library is built in-tree (``python onion_gen_b200/build.py``). There is no
+fallback: if it is missing or does not load, importing this module raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libonion_gen_b200.so")
+
+OG_OK = 0
+STATUS = {
+    0: "OG_OK",
+    1: "OG_E_ARG",
+    2: "OG_E_NODEVICE",
+    3: "OG_E_DEVICE",
+    4: "OG_E_NOMEM",
+    5: "OG_E_OVERFLOW",
+    6: "OG_E_CAPACITY",
+    7: "OG_E_FILTER",
+    8: "OG_E_STATE",
+    9: "OG_E_TIMEOUT",
+    10: "OG_E_VERIFY",
+}
+SCHEME_PAIRED = 0
+SCHEME_CHAIN = 1
+
+
+class OgError(RuntimeError):
+    """A nonzero og_status with its message."""
+
+    def __init__(self, code: int, message: str):
+        self.code = code
+        self.status = STATUS.get(code, str(code))
+        super().__init__(f"{self.status}: {message}")
+
+
+class Survivor(C.Structure):
+    _fields_ = [("offset", C.c_uint64), ("packed", C.c_uint8 * 32)]
+
+
+class EngineConfig(C.Structure):
+    _fields_ = [
+        ("scheme", C.c_uint32),
+        ("half", C.c_uint32),
+        ("lanes", C.c_uint32),
+        ("rounds", C.c_uint32),
+        ("block", C.c_uint32),
+        ("dump", C.c_uint32),
+        ("room", C.c_uint32),
+    ]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python onion_gen_b200/build.py` "
+            "(there is no CPU fallback for the device engine)"
+        )
+    L = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    B = C.c_char_p
+    SZ = C.c_size_t
+    U32, U64 = C.c_uint32, C.c_uint64
+    I = C.c_int
+
+    def sig(name, res, args):
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+
+    sig("og_device_count", I, [C.POINTER(I), B, SZ])
+    sig("og_device_info", I, [I, B, SZ, C.POINTER(U64), C.POINTER(I), B, SZ])
+    sig("og_engine_new", I, [I, B, U32, P, SZ, U32, I, C.POINTER(P), B, SZ])
+    sig("og_engine_new_config", I, [I, B, C.POINTER(EngineConfig), P, SZ, U32, C.POINTER(P), B, SZ])
+    sig("og_engine_threads", U32, [P])
+    sig("og_engine_batch", U64, [P])
+    sig("og_engine_room", SZ, [P])
+    sig("og_engine_shape", None, [P, C.POINTER(EngineConfig)])
+    sig("og_engine_advance", I, [P, P, SZ, C.POINTER(SZ), B, SZ])
+    sig("og_engine_last_kernel_ms", C.c_float, [P])
+    sig("og_engine_free", None, [P])
+    sig("og_measure_int_peak", I, [I, C.POINTER(C.c_double), C.POINTER(C.c_double), B, SZ])
+    sig("og_secret_scalar", None, [B, B])
+    sig("og_expanded_secret_key", None, [B, B])
+    sig("og_expanded_secret_at_offset", I, [B, U64, B])
+    sig("og_scalar_base_mult", None, [B, B])
+    sig("og_pack", None, [B, B])
+    sig("og_address", None, [B, B])
+    sig("og_block_seed", None, [B, U64, B])
+    sig("og_check_hit", I, [B, U64, B, B, B])
+    sig("og_filters_new", I, [B, U32, C.POINTER(P), B, SZ])
+    sig("og_filters_count", SZ, [P])
+    sig("og_filters_text", I, [P, SZ, B, SZ])
+    sig("og_filters_bits", U32, [P])
+    sig("og_filters_words", SZ, [P, C.POINTER(C.POINTER(U64))])
+    sig("og_filters_occupancy", C.c_double, [P])
+    sig("og_filters_match", C.c_long, [P, B])
+    sig("og_filters_free", None, [P])
+    return L
+
+
+lib = _load()
+
+
+def errbuf():
+    return C.create_string_buffer(512)
+
+
+def check(code: int, err) -> None:
+    if code != OG_OK:
+        raise OgError(code, err.value.decode(errors="replace"))

@@ -1,0 +1,485 @@
+// og_engine: the single-search device engine behind the C ABI.
+//
+// Mirrors cuda::Engine (src/gpu/cuda.rs:103-365) and the shape logic of
+// gpu::Engine (src/gpu/mod.rs:292-477): host precompute once, lane state
+// resident in HBM, one kernel launch per advance, one synchronisation, a
+// copy of only the survivors that were written, and an overflow that is an
+// error rather than a truncation.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/onion_gen_b200.h"
+#include "host/common.h"
+#include "host/filters.h"
+#include "host/tuning.h"
+#include "kernels.cuh"
+
+using namespace og;
+
+namespace og {
+
+// Affine x, y of many points with one inversion (Montgomery).
+static void batch_affine(const std::vector<Pt>& pts, std::vector<F51>& xs, std::vector<F51>& ys) {
+    const size_t n = pts.size();
+    std::vector<F51> prefix(n);
+    F51 run = f_one();
+    for (size_t i = 0; i < n; i++) {
+        prefix[i] = run;
+        run = f_mul(run, pts[i].Z);
+    }
+    F51 inv = f_inv(run);
+    xs.resize(n);
+    ys.resize(n);
+    for (size_t i = n; i-- > 0;) {
+        const F51 zi = f_mul(inv, prefix[i]);
+        inv = f_mul(inv, pts[i].Z);
+        xs[i] = f_mul(pts[i].X, zi);
+        ys[i] = f_mul(pts[i].Y, zi);
+    }
+}
+
+// The table Q_m = 8m G, m = 1..half, affine (x, y, xy), in the device
+// layout; the same for every search, so built once per half.
+const std::vector<uint4>& pair_table(uint32_t half) {
+    static std::mutex mu;
+    static std::map<uint32_t, std::unique_ptr<std::vector<uint4>>> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(half);
+    if (it != cache.end()) return *it->second;
+    std::vector<Pt> pts(half);
+    const Pt eight = base_mult_u64(8);
+    Pt p = eight;
+    for (uint32_t m = 0; m < half; m++) {
+        pts[m] = p;
+        p = pt_add(p, eight);
+    }
+    std::vector<F51> xs, ys;
+    batch_affine(pts, xs, ys);
+    auto v = std::make_unique<std::vector<uint4>>((size_t)half * 6);
+    for (uint32_t m = 0; m < half; m++) {
+        uint4* d = v->data() + (size_t)m * 6;
+        put_fe(d + 0, 1, xs[m]);
+        put_fe(d + 2, 1, ys[m]);
+        put_fe(d + 4, 1, f_mul(xs[m], ys[m]));
+    }
+    auto& ref = *v;
+    cache[half] = std::move(v);
+    return ref;
+}
+
+// 2^k * stride for k < nbits in cached form (y+x, y-x, 2dxy), device layout.
+std::vector<uint4> pow2_table(const Pt& stride, uint32_t nbits) {
+    std::vector<uint4> out((size_t)std::max<uint32_t>(nbits, 1) * 6);
+    Pt p = stride;
+    for (uint32_t k = 0; k < nbits; k++) {
+        const Niels c = pt_niels(p);
+        uint4* d = out.data() + (size_t)k * 6;
+        put_fe(d + 0, 1, c.ypx);
+        put_fe(d + 2, 1, c.ymx);
+        put_fe(d + 4, 1, c.xy2d);
+        p = pt_dbl(p);
+    }
+    return out;
+}
+
+uint32_t bits_for(uint64_t v) {
+    uint32_t b = 0;
+    while (b < 64 && (v >> b) != 0) b++;
+    return b;
+}
+
+}  // namespace og
+
+struct og_engine {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    og_engine_config cfg{};
+    uint32_t slots = 0;
+    uint32_t bits = 0;
+    size_t cap = 0;
+    uint64_t launches = 0;
+    float last_ms = 0;
+    bool overflowed = false;
+    DevBuf<uint4> lanes, scratch, table, pow2;
+    DevBuf<uint32_t> bitmap, counter;
+    DevBuf<HitRec> hits;
+    HostBuf<HitRec> h_hits;
+    HostBuf<uint32_t> h_counter;
+    PairedArgs pa{};
+    ChainArgs ca{};
+
+    ~og_engine() {
+        if (stream) {
+            cudaStreamSynchronize(stream);
+            cudaStreamDestroy(stream);
+        }
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+    }
+};
+
+namespace {
+
+#define CU(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t _e = (call);                                                              \
+        if (_e != cudaSuccess)                                                                \
+            return fail(err, errlen, _e == cudaErrorMemoryAllocation ? OG_E_NOMEM : OG_E_DEVICE, \
+                        "%s: %s", #call, cuda_text(_e).c_str());                              \
+    } while (0)
+
+int resident_lanes(int device, uint32_t scheme, uint32_t half, uint32_t block, uint32_t* out, char* err,
+                   size_t errlen) {
+    KernelInfo info{};
+    cudaError_t e = scheme == OG_SCHEME_CHAIN ? chain_info((int)block, &info) : paired_info((int)block, half, &info);
+    if (e != cudaSuccess) return fail(err, errlen, OG_E_DEVICE, "kernel attributes: %s", cuda_text(e).c_str());
+    int sms = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return fail(err, errlen, OG_E_DEVICE, "device attributes: %s", cuda_text(e).c_str());
+    *out = (uint32_t)std::max(1, info.blocks_per_sm) * (uint32_t)sms * block;
+    return OG_OK;
+}
+
+// Records one advance may produce: every candidate in dump mode; else four
+// times what the bitmap's measured occupancy lets through plus a floor
+// (the margin of src/gpu/mod.rs:298-312, taken from the real occupancy
+// rather than one slot per prefix, so that short prefixes cannot overflow).
+size_t room_for(uint64_t batch, bool dump, double occupancy) {
+    if (dump) return (size_t)batch;
+    const double expected = (double)batch * occupancy;
+    const double want = 4.0 * expected + 1024.0;
+    return (size_t)std::min<double>((double)batch, std::max(4096.0, want));
+}
+
+int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, const uint64_t* bitmap, size_t words,
+                 uint32_t bits, og_engine** out, char* err, size_t errlen) {
+    if (!out || !start) return fail(err, errlen, OG_E_ARG, "null argument");
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+        return fail(err, errlen, OG_E_NODEVICE, "no CUDA device is available");
+    if (ordinal < 0 || ordinal >= count) return fail(err, errlen, OG_E_ARG, "device %d of %d", ordinal, count);
+    if (cfg.scheme > OG_SCHEME_CHAIN) return fail(err, errlen, OG_E_ARG, "unknown scheme %u", cfg.scheme);
+    if (!cfg.dump) {
+        if (!bitmap) return fail(err, errlen, OG_E_ARG, "no bitmap: without one every candidate would cross back");
+        if (bits < 8 || bits > 32) return fail(err, errlen, OG_E_ARG, "bitmap width %u outside 8..32", bits);
+        const size_t need = (size_t)(((1ULL << bits) + 63) / 64);
+        if (words < need) return fail(err, errlen, OG_E_ARG, "%zu words for a %u-bit index (%zu needed)", words, bits, need);
+    }
+    CU(cudaSetDevice(ordinal));
+    if (cfg.block == 0) cfg.block = 128;
+    if (cfg.block % 32 || cfg.block > 256) return fail(err, errlen, OG_E_ARG, "block %u (a multiple of 32, at most 256)", cfg.block);
+    if (cfg.half == 0) cfg.half = cfg.scheme == OG_SCHEME_CHAIN ? 256 : 128;
+    if (cfg.scheme == OG_SCHEME_PAIRED && cfg.half > 2048) return fail(err, errlen, OG_E_ARG, "half %u > 2048", cfg.half);
+    if (cfg.scheme == OG_SCHEME_CHAIN && cfg.half > 65536) return fail(err, errlen, OG_E_ARG, "n %u > 65536", cfg.half);
+    if (cfg.lanes == 0) {
+        int rc = resident_lanes(ordinal, cfg.scheme, cfg.half, cfg.block, &cfg.lanes, err, errlen);
+        if (rc) return rc;
+    }
+    cfg.lanes = (cfg.lanes + cfg.block - 1) / cfg.block * cfg.block;
+    if (cfg.lanes > (1u << 24)) return fail(err, errlen, OG_E_ARG, "%u lanes (at most 2^24)", cfg.lanes);
+    const uint32_t slots = cfg.scheme == OG_SCHEME_CHAIN ? cfg.half : 2 * cfg.half + 1;
+    if (cfg.rounds == 0) {
+        const uint64_t per_round = (uint64_t)cfg.lanes * slots;
+        cfg.rounds = (uint32_t)std::max<uint64_t>(1, (1ULL << 27) / per_round);
+    }
+    double occupancy = 1.0;
+    if (!cfg.dump) {
+        std::vector<uint64_t> w(bitmap, bitmap + (size_t)(((1ULL << bits) + 63) / 64));
+        occupancy = bitmap_occupancy(w, bits);
+        // keep the survivor buffer of one advance within 2^24 records
+        while (cfg.rounds > 1 && 4.0 * (double)cfg.lanes * slots * cfg.rounds * occupancy > (double)(1u << 24))
+            cfg.rounds /= 2;
+    }
+    if ((uint64_t)cfg.rounds * slots > 0xffffffffULL) return fail(err, errlen, OG_E_ARG, "too many rounds per advance");
+
+    Pt start_pt = point_from_bytes(start);
+    if (!point_valid(start_pt)) return fail(err, errlen, OG_E_ARG, "the start point is not on the curve");
+
+    std::unique_ptr<og_engine> e(new (std::nothrow) og_engine());
+    if (!e) return fail(err, errlen, OG_E_NOMEM, "host memory");
+    e->device = ordinal;
+    e->cfg = cfg;
+    e->slots = slots;
+    e->bits = bits;
+    CU(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    CU(cudaEventCreate(&e->ev0));
+    CU(cudaEventCreate(&e->ev1));
+
+    const size_t L = cfg.lanes;
+    const uint64_t batch = (uint64_t)L * slots * cfg.rounds;
+    e->cap = cfg.room ? cfg.room : room_for(batch, cfg.dump != 0, occupancy);
+    e->cfg.room = (uint32_t)std::min<size_t>(e->cap, 0xffffffffu);
+    const uint32_t coords = cfg.scheme == OG_SCHEME_CHAIN ? 4 : 2;
+    CU(e->lanes.alloc(L * coords * 2));
+    const size_t elems = cfg.scheme == OG_SCHEME_CHAIN ? cfg.half : 2 * (size_t)cfg.half + 2;
+    CU(e->scratch.alloc(L * elems * 4));
+    CU(e->counter.alloc(1));
+    CU(e->hits.alloc(e->cap));
+    CU(e->h_hits.alloc(e->cap));
+    CU(e->h_counter.alloc(1));
+    if (!cfg.dump) {
+        const size_t w32 = (size_t)(((1ULL << bits) + 31) / 32);
+        CU(e->bitmap.alloc(std::max<size_t>(w32, 2)));
+        CU(cudaMemcpyAsync(e->bitmap.p, bitmap, w32 * 4, cudaMemcpyHostToDevice, e->stream));
+    }
+
+    // lane start points
+    InitArgs ia{};
+    Pt base, stride;
+    if (cfg.scheme == OG_SCHEME_PAIRED) {
+        base = pt_add(start_pt, base_mult_u64(8ULL * (cfg.half + 1)));  // first centre
+        stride = base_mult_u64(8ULL * slots);
+        ia.affine_out = 1;
+    } else {
+        base = start_pt;
+        stride = base_mult_u64(8ULL * slots);
+        ia.affine_out = 0;
+    }
+    const uint32_t nbits = bits_for(L - 1);
+    std::vector<uint4> pw = pow2_table(stride, nbits);
+    CU(e->pow2.alloc(pw.size()));
+    CU(cudaMemcpyAsync(e->pow2.p, pw.data(), pw.size() * sizeof(uint4), cudaMemcpyHostToDevice, e->stream));
+    ia.lanes = e->lanes.p;
+    ia.bx = to_words(base.X);
+    ia.by = to_words(base.Y);
+    ia.bz = to_words(base.Z);
+    ia.bt = to_words(base.T);
+    ia.pow2 = e->pow2.p;
+    ia.nbits = nbits;
+    ia.lanes_n = cfg.lanes;
+    CU(launch_init(ia, 128, e->stream));
+
+    if (cfg.scheme == OG_SCHEME_PAIRED) {
+        const std::vector<uint4>& tab = pair_table(cfg.half);
+        CU(e->table.alloc(tab.size()));
+        CU(cudaMemcpyAsync(e->table.p, tab.data(), tab.size() * sizeof(uint4), cudaMemcpyHostToDevice, e->stream));
+        F51 wx, wy;
+        pt_affine(base_mult_u64(8ULL * slots * L), wx, wy);
+        PairedArgs& a = e->pa;
+        a.table = e->table.p;
+        a.lanes = e->lanes.p;
+        a.scratch = e->scratch.p;
+        a.bitmap = cfg.dump ? nullptr : e->bitmap.p;
+        a.bits = bits;
+        a.hits = e->hits.p;
+        a.counter = e->counter.p;
+        a.cap = (uint32_t)std::min<size_t>(e->cap, 0xffffffffu);
+        a.search = 0;
+        a.wx = to_words(wx);
+        a.wy = to_words(wy);
+        a.wt = to_words(f_mul(wx, wy));
+        a.lanes_n = cfg.lanes;
+        a.half = cfg.half;
+        a.rounds = cfg.rounds;
+    } else {
+        const Niels step = pt_niels(base_mult_u64(8));
+        ChainArgs& a = e->ca;
+        a.lanes = e->lanes.p;
+        a.scratch = e->scratch.p;
+        a.bitmap = cfg.dump ? nullptr : e->bitmap.p;
+        a.bits = bits;
+        a.hits = e->hits.p;
+        a.counter = e->counter.p;
+        a.cap = (uint32_t)std::min<size_t>(e->cap, 0xffffffffu);
+        a.search = 0;
+        a.step_ypx = to_words(step.ypx);
+        a.step_ymx = to_words(step.ymx);
+        a.step_t2d = to_words(step.xy2d);
+        if (L > 1) {
+            const Niels jump = pt_niels(base_mult_u64(8ULL * (L - 1) * slots));
+            a.jump_ypx = to_words(jump.ypx);
+            a.jump_ymx = to_words(jump.ymx);
+            a.jump_t2d = to_words(jump.xy2d);
+        }
+        a.lanes_n = cfg.lanes;
+        a.n = cfg.half;
+        a.rounds = cfg.rounds;
+    }
+    CU(cudaStreamSynchronize(e->stream));
+    *out = e.release();
+    return OG_OK;
+}
+
+// One advance timed on the device, candidates per second (the method of
+// gpu::Engine::time_one_launch, src/gpu/mod.rs:420-428, on CUDA events).
+double time_advance(og_engine* e, std::vector<og_survivor>& buf) {
+    size_t n = 0;
+    if (og_engine_advance(e, buf.data(), buf.size(), &n, nullptr, 0) != OG_OK) return -1;
+    if (og_engine_advance(e, buf.data(), buf.size(), &n, nullptr, 0) != OG_OK) return -1;
+    const double ms = e->last_ms;
+    return ms > 0 ? (double)og_engine_batch(e) / (ms * 1e-3) : -1;
+}
+
+}  // namespace
+
+extern "C" {
+
+int og_device_count(int* count, char* err, size_t errlen) {
+    if (!count) return fail(err, errlen, OG_E_ARG, "null argument");
+    *count = 0;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e == cudaErrorNoDevice || (e == cudaSuccess && n == 0))
+        return fail(err, errlen, OG_E_NODEVICE, "the driver reports no device");
+    if (e != cudaSuccess) return fail(err, errlen, OG_E_NODEVICE, "no usable CUDA driver (%s)", cuda_text(e).c_str());
+    *count = n;
+    return OG_OK;
+}
+
+int og_device_info(int ordinal, char* name, size_t namelen, uint64_t* memory, int* sms, char* err, size_t errlen) {
+    cudaDeviceProp p;
+    cudaError_t e = cudaGetDeviceProperties(&p, ordinal);
+    if (e != cudaSuccess) return fail(err, errlen, OG_E_DEVICE, "device %d: %s", ordinal, cuda_text(e).c_str());
+    if (name && namelen) snprintf(name, namelen, "%s", p.name);
+    if (memory) *memory = p.totalGlobalMem;
+    if (sms) *sms = p.multiProcessorCount;
+    return OG_OK;
+}
+
+int og_engine_new_config(int ordinal, const uint8_t start[128], const og_engine_config* cfg, const uint64_t* bitmap,
+                         size_t words, uint32_t bits, og_engine** out, char* err, size_t errlen) {
+    og_engine_config c{};
+    if (cfg) c = *cfg;
+    return build_engine(ordinal, start, c, bitmap, words, bits, out, err, errlen);
+}
+
+int og_engine_new(int ordinal, const uint8_t start[128], uint32_t threads, const uint64_t* bitmap, size_t words,
+                  uint32_t bits, int retune, og_engine** out, char* err, size_t errlen) {
+    og_engine_config cfg{};
+    cfg.scheme = OG_SCHEME_PAIRED;
+    if (threads != 0) {
+        cfg.lanes = threads;
+        return build_engine(ordinal, start, cfg, bitmap, words, bits, out, err, errlen);
+    }
+    char name[256] = "unnamed";
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, ordinal) == cudaSuccess) snprintf(name, sizeof name, "%s", p.name);
+    const std::string key = device_key(name, "cuda", 0);
+    Shape shape;
+    if (!retune && tuning_get(key, shape) && shape.first && shape.second) {
+        cfg.half = shape.first;
+        cfg.lanes = shape.second;
+        cfg.block = shape.block;
+        cfg.rounds = shape.rounds;
+        if (build_engine(ordinal, start, cfg, bitmap, words, bits, out, err, errlen) == OG_OK) return OG_OK;
+        // the remembered shape no longer builds: measure again
+    }
+    // Timed walk over inversion batch and lanes in flight; the fastest is
+    // kept and recorded (src/gpu/mod.rs:383-411).
+    og_engine* best = nullptr;
+    double best_rate = -1;
+    int last = OG_E_DEVICE;
+    for (uint32_t half : {64u, 128u, 256u}) {
+        uint32_t resident = 0;
+        if (resident_lanes(ordinal, OG_SCHEME_PAIRED, half, 128, &resident, err, errlen) != OG_OK) continue;
+        for (uint32_t mult : {1u, 2u, 4u}) {
+            og_engine_config c{};
+            c.scheme = OG_SCHEME_PAIRED;
+            c.half = half;
+            c.lanes = resident * mult;
+            c.block = 128;
+            og_engine* e = nullptr;
+            last = build_engine(ordinal, start, c, bitmap, words, bits, &e, err, errlen);
+            if (last != OG_OK) continue;
+            std::vector<og_survivor> buf(og_engine_room(e));
+            const double rate = time_advance(e, buf);
+            if (rate > best_rate) {
+                if (best) og_engine_free(best);
+                best = e;
+                best_rate = rate;
+            } else {
+                og_engine_free(e);
+            }
+        }
+    }
+    if (!best) return fail(err, errlen, last, "no launch shape this device would take");
+    Shape s;
+    s.first = best->cfg.half;
+    s.second = best->cfg.lanes;
+    s.block = best->cfg.block;
+    s.rounds = best->cfg.rounds;
+    s.rate = best_rate;
+    s.at = unix_now();
+    tuning_put(key, s);
+    // hand back a fresh engine at the chosen shape: the timed one has moved on
+    og_engine_config c = best->cfg;
+    og_engine_free(best);
+    return build_engine(ordinal, start, c, bitmap, words, bits, out, err, errlen);
+}
+
+uint32_t og_engine_threads(const og_engine* e) { return e ? e->cfg.lanes : 0; }
+
+uint64_t og_engine_batch(const og_engine* e) {
+    return e ? (uint64_t)e->cfg.lanes * e->slots * e->cfg.rounds : 0;
+}
+
+size_t og_engine_room(const og_engine* e) { return e ? e->cap : 0; }
+
+void og_engine_shape(const og_engine* e, og_engine_config* cfg) {
+    if (e && cfg) *cfg = e->cfg;
+}
+
+float og_engine_last_kernel_ms(const og_engine* e) { return e ? e->last_ms : 0.f; }
+
+int og_engine_advance(og_engine* e, og_survivor* out, size_t cap, size_t* n, char* err, size_t errlen) {
+    if (!e || !n) return fail(err, errlen, OG_E_ARG, "null argument");
+    *n = 0;
+    if (e->overflowed) return fail(err, errlen, OG_E_STATE, "an earlier advance overflowed; the engine is closed");
+    CU(cudaSetDevice(e->device));
+    CU(cudaMemsetAsync(e->counter.p, 0, sizeof(uint32_t), e->stream));
+    CU(cudaEventRecord(e->ev0, e->stream));
+    if (e->cfg.scheme == OG_SCHEME_PAIRED) {
+        CU(launch_paired(e->pa, (int)e->cfg.block, e->stream));
+    } else {
+        CU(launch_chain(e->ca, (int)e->cfg.block, e->stream));
+    }
+    CU(cudaEventRecord(e->ev1, e->stream));
+    CU(cudaMemcpyAsync(e->h_counter.p, e->counter.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream));
+    CU(cudaStreamSynchronize(e->stream));
+    cudaEventElapsedTime(&e->last_ms, e->ev0, e->ev1);
+    const uint64_t launch = e->launches++;
+    const uint32_t found = *e->h_counter.p;
+    if (found > e->cap) {
+        e->overflowed = true;
+        return fail(err, errlen, OG_E_OVERFLOW,
+                    "one advance produced %u survivors and only %zu fit; the index is too narrow for what it "
+                    "is filtering: a wider index is the answer",
+                    found, e->cap);
+    }
+    if (found > cap)
+        return fail(err, errlen, OG_E_CAPACITY, "%u survivors and room for %zu in the caller's buffer", found, cap);
+    if (found) {
+        CU(cudaMemcpyAsync(e->h_hits.p, e->hits.p, (size_t)found * sizeof(HitRec), cudaMemcpyDeviceToHost, e->stream));
+        CU(cudaStreamSynchronize(e->stream));
+    }
+    const uint64_t L = e->cfg.lanes, slots = e->slots, R = e->cfg.rounds;
+    const bool paired = e->cfg.scheme == OG_SCHEME_PAIRED;
+    for (uint32_t k = 0; k < found; k++) {
+        const HitRec& h = e->h_hits.p[k];
+        const uint64_t r = h.step / slots, i = h.step % slots;
+        const uint64_t w = (launch * R + r) * L + h.lane;
+        out[k].offset = paired ? 8 * (w * slots + 1 + i) : 8 * (w * slots + i);
+        for (int j = 0; j < 8; j++) {
+            out[k].packed[4 * j + 0] = (uint8_t)(h.y[j]);
+            out[k].packed[4 * j + 1] = (uint8_t)(h.y[j] >> 8);
+            out[k].packed[4 * j + 2] = (uint8_t)(h.y[j] >> 16);
+            out[k].packed[4 * j + 3] = (uint8_t)(h.y[j] >> 24);
+        }
+    }
+    *n = found;
+    return OG_OK;
+}
+
+void og_engine_free(og_engine* e) { delete e; }
+
+}  // extern "C"

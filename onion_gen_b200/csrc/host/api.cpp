@@ -1,0 +1,108 @@
+// C ABI of the host side of the hit path: keys, re-derivation, filters.
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../../include/onion_gen_b200.h"
+#include "common.h"
+#include "filters.h"
+#include "keys.h"
+
+using namespace og;
+
+struct og_filters {
+    FilterSet set;
+};
+
+extern "C" {
+
+void og_secret_scalar(const uint8_t seed[32], uint8_t scalar[32]) { secret_scalar(seed, scalar); }
+
+void og_expanded_secret_key(const uint8_t seed[32], uint8_t out[64]) { expanded_secret_key(seed, out); }
+
+int og_expanded_secret_at_offset(const uint8_t seed[32], uint64_t offset, uint8_t out[64]) {
+    return expanded_secret_at_offset(seed, offset, out) ? 1 : 0;
+}
+
+void og_scalar_base_mult(const uint8_t scalar[32], uint8_t point[128]) { point_to_bytes(base_mult(scalar), point); }
+
+void og_pack(const uint8_t point[128], uint8_t out[32]) { pt_encode(point_from_bytes(point), out); }
+
+void og_address(const uint8_t pk[32], char out[57]) {
+    const std::string a = address(pk);
+    std::memcpy(out, a.c_str(), 57);
+}
+
+void og_block_seed(const uint8_t root[32], uint64_t index, uint8_t out[32]) { block_seed(root, index, out); }
+
+int og_check_hit(const uint8_t seed[32], uint64_t offset, const uint8_t packed[32], uint8_t pk[32], uint8_t secret[64]) {
+    uint8_t p[32], s[64];
+    switch (check_hit(seed, offset, packed, p, s)) {
+        case HitCheck::ok:
+            if (pk) std::memcpy(pk, p, 32);
+            if (secret) std::memcpy(secret, s, 64);
+            return OG_OK;
+        case HitCheck::clamping:
+            return OG_E_ARG;
+        default:
+            return OG_E_VERIFY;
+    }
+}
+
+int og_filters_new(const char* text, uint32_t bits, og_filters** out, char* err, size_t errlen) {
+    if (!text || !out) return fail(err, errlen, OG_E_ARG, "null argument");
+    *out = nullptr;
+    std::vector<PrefixFilter> fs;
+    const char* p = text;
+    size_t line = 0;
+    while (*p) {
+        const char* e = std::strchr(p, '\n');
+        std::string s = e ? std::string(p, (size_t)(e - p)) : std::string(p);
+        line++;
+        bool blank = true;
+        for (char c : s)
+            if (c != ' ' && c != '\t' && c != '\r') blank = false;
+        if (!blank) {
+            PrefixFilter f;
+            std::string why;
+            if (!parse_prefix(s, f, why)) return fail(err, errlen, OG_E_FILTER, "line %zu: %s", line, why.c_str());
+            fs.push_back(f);
+        }
+        if (!e) break;
+        p = e + 1;
+    }
+    og_filters* h = new (std::nothrow) og_filters();
+    if (!h) return fail(err, errlen, OG_E_NOMEM, "host memory");
+    std::string why;
+    if (!h->set.build(std::move(fs), bits, why)) {
+        delete h;
+        return fail(err, errlen, OG_E_FILTER, "%s", why.c_str());
+    }
+    *out = h;
+    return OG_OK;
+}
+
+size_t og_filters_count(const og_filters* f) { return f ? f->set.size() : 0; }
+
+int og_filters_text(const og_filters* f, size_t i, char* out, size_t cap) {
+    if (!f || i >= f->set.size() || !out || cap == 0) return OG_E_ARG;
+    snprintf(out, cap, "%s", f->set.filter(i).text.c_str());
+    return OG_OK;
+}
+
+uint32_t og_filters_bits(const og_filters* f) { return f ? f->set.bits() : 0; }
+
+size_t og_filters_words(const og_filters* f, const uint64_t** words) {
+    if (!f) return 0;
+    if (words) *words = f->set.words().data();
+    return f->set.words().size();
+}
+
+double og_filters_occupancy(const og_filters* f) { return f ? f->set.occupancy() : 0.0; }
+
+long og_filters_match(const og_filters* f, const uint8_t packed[32]) { return f ? f->set.match_key(packed) : -1; }
+
+void og_filters_free(og_filters* f) { delete f; }
+
+}  // extern "C"

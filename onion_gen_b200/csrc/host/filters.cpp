@@ -1,0 +1,225 @@
+#include "filters.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "keys.h"
+
+namespace og {
+
+namespace {
+
+std::string trim(const std::string& s) {
+    size_t a = 0, b = s.size();
+    while (a < b && (s[a] == ' ' || s[a] == '\t' || s[a] == '\r' || s[a] == '\n')) a++;
+    while (b > a && (s[b - 1] == ' ' || s[b - 1] == '\t' || s[b - 1] == '\r' || s[b - 1] == '\n')) b--;
+    return s.substr(a, b - a);
+}
+
+uint64_t head64(const uint8_t packed[32]) {
+    uint64_t v = 0;
+    for (int i = 0; i < 8; i++) v = (v << 8) | packed[i];
+    return v;
+}
+
+// top `bits` bits of the packed key, big-endian (src/filter.rs:2538-2549)
+size_t slot_of(const uint8_t packed[32], uint32_t bits) { return (size_t)(head64(packed) >> (64 - bits)); }
+
+}  // namespace
+
+bool PrefixFilter::matches_key(const uint8_t packed[32]) const {
+    const size_t last = nbytes - 1;
+    return std::memcmp(packed, bytes, last) == 0 && (packed[last] & mask) == bytes[last];
+}
+
+bool parse_prefix(const std::string& raw, PrefixFilter& out, std::string& err) {
+    std::string s = trim(raw);
+    const size_t colon = s.find(':');
+    if (colon != std::string::npos) {
+        std::string form = trim(s.substr(0, colon));
+        for (char& c : form) c = (char)std::tolower((unsigned char)c);
+        if (form != "prefix") {
+            err = "the " + form + " form is not supported by the device engine; only literal prefixes are";
+            return false;
+        }
+        s = trim(s.substr(colon + 1));
+    } else {
+        size_t k = 0;
+        while (k < s.size() && s[k] == '^') k++;
+        s = s.substr(k);
+    }
+    if (s.empty()) {
+        err = "the filter is empty";
+        return false;
+    }
+    if (s.size() > ADDRESS_SYMBOLS) {
+        err = "a filter of " + std::to_string(s.size()) + " symbols is longer than an address (56)";
+        return false;
+    }
+    std::string canon;
+    for (size_t i = 0; i < s.size(); i++) {
+        const int v = base32_value(s[i]);
+        if (v < 0) {
+            err = std::string("invalid character '") + s[i] + "' at position " + std::to_string(i) +
+                  ": the base32 alphabet is a-z and 2-7";
+            return false;
+        }
+        canon.push_back(BASE32_ALPHABET[v]);
+    }
+    out.text = canon;
+    // decode the first min(len, 49) symbols into bytes plus a mask for the
+    // partly significant last byte (src/filter.rs:649-685)
+    const size_t sym = std::min(canon.size(), KEY_ONLY_SYMBOLS);
+    const size_t bits = sym * 5;
+    std::memset(out.bytes, 0, sizeof out.bytes);
+    for (size_t i = 0; i < sym; i++) {
+        const unsigned v = (unsigned)base32_value(canon[i]);
+        for (unsigned k = 0; k < 5; k++) {
+            const size_t b = i * 5 + k;
+            if ((v >> (4 - k)) & 1) out.bytes[b / 8] |= (uint8_t)(0x80 >> (b % 8));
+        }
+    }
+    out.nbytes = (bits + 7) / 8;
+    const unsigned rem = bits % 8;
+    out.mask = rem == 0 ? 0xff : (uint8_t)(0xff << (8 - rem));
+    out.bytes[out.nbytes - 1] &= out.mask;
+    return true;
+}
+
+std::vector<uint64_t> build_bitmap(const std::vector<PrefixFilter>& filters, uint32_t bits) {
+    std::vector<uint64_t> words;
+    if (filters.empty() || bits < 8 || bits > 32) return words;
+    words.assign((size_t)(((1ULL << bits) + 63) / 64), 0);
+    for (const PrefixFilter& f : filters) {
+        const size_t sym = std::min(f.text.size(), KEY_ONLY_SYMBOLS);
+        const uint32_t pbits = (uint32_t)(sym * 5);
+        uint8_t probe[32] = {0};
+        std::memcpy(probe, f.bytes, f.nbytes);
+        const size_t first = slot_of(probe, bits);
+        const size_t run = pbits >= bits ? 1 : (size_t)1 << (bits - pbits);
+        // whole words where the run covers them, bits at the ends
+        size_t s = first;
+        const size_t end = first + run;
+        while (s < end && (s & 63)) {
+            words[s >> 6] |= 1ULL << (s & 63);
+            s++;
+        }
+        while (s + 64 <= end) {
+            words[s >> 6] = ~0ULL;
+            s += 64;
+        }
+        while (s < end) {
+            words[s >> 6] |= 1ULL << (s & 63);
+            s++;
+        }
+    }
+    if (bitmap_occupancy(words, bits) > 0.25) words.clear();
+    return words;
+}
+
+double bitmap_occupancy(const std::vector<uint64_t>& words, uint32_t bits) {
+    uint64_t set = 0;
+    for (uint64_t w : words) set += (uint64_t)__builtin_popcountll(w);
+    return (double)set / (double)(1ULL << bits);
+}
+
+bool FilterSet::build(std::vector<PrefixFilter> filters, uint32_t bits, std::string& err) {
+    std::sort(filters.begin(), filters.end(),
+              [](const PrefixFilter& a, const PrefixFilter& b) { return a.text < b.text; });
+    filters_.clear();
+    for (PrefixFilter& f : filters) {
+        if (!filters_.empty() && f.text.compare(0, filters_.back().text.size(), filters_.back().text) == 0) continue;
+        filters_.push_back(f);
+    }
+    if (filters_.empty()) {
+        err = "no filters";
+        return false;
+    }
+    if (bits == 0) {
+        std::vector<uint64_t> widest;
+        uint32_t widest_bits = 0;
+        for (uint32_t b = 16; b <= 24; b++) {
+            std::vector<uint64_t> w = build_bitmap(filters_, b);
+            if (w.empty()) continue;
+            const bool good = bitmap_occupancy(w, b) <= 0.01;
+            widest.swap(w);
+            widest_bits = b;
+            if (good) break;
+        }
+        words_.swap(widest);
+        bits_ = widest_bits;
+    } else {
+        if (bits < 8 || bits > 32) {
+            err = "the index width must be 8..32 bits";
+            return false;
+        }
+        words_ = build_bitmap(filters_, bits);
+        bits_ = bits;
+    }
+    if (words_.empty()) {
+        err = "the filters fill more than a quarter of every index width; no bitmap can discriminate";
+        return false;
+    }
+    // length buckets for the exact match
+    buckets_.clear();
+    for (size_t i = 0; i < filters_.size(); i++) {
+        const size_t sym = std::min(filters_[i].text.size(), KEY_ONLY_SYMBOLS);
+        auto it = std::find_if(buckets_.begin(), buckets_.end(), [&](const Bucket& b) { return b.symbols == sym; });
+        if (it == buckets_.end()) {
+            Bucket b;
+            b.symbols = sym;
+            const unsigned hb = (unsigned)std::min<size_t>(sym * 5, 64);
+            b.mask = hb == 64 ? ~0ULL : ~0ULL << (64 - hb);
+            buckets_.push_back(b);
+            it = buckets_.end() - 1;
+        }
+        uint8_t padded[32] = {0};
+        std::memcpy(padded, filters_[i].bytes, filters_[i].nbytes);
+        it->keys.push_back(head64(padded) & it->mask);
+        it->owners.push_back((uint32_t)i);
+    }
+    for (Bucket& b : buckets_) {
+        std::vector<size_t> order(b.keys.size());
+        for (size_t k = 0; k < order.size(); k++) order[k] = k;
+        std::sort(order.begin(), order.end(), [&](size_t x, size_t y) { return b.keys[x] < b.keys[y]; });
+        std::vector<uint64_t> keys(order.size());
+        std::vector<uint32_t> owners(order.size());
+        for (size_t k = 0; k < order.size(); k++) {
+            keys[k] = b.keys[order[k]];
+            owners[k] = b.owners[order[k]];
+        }
+        b.keys.swap(keys);
+        b.owners.swap(owners);
+    }
+    return true;
+}
+
+double FilterSet::occupancy() const { return bitmap_occupancy(words_, bits_); }
+
+bool FilterSet::may_match(const uint8_t packed[32]) const {
+    const size_t s = slot_of(packed, bits_);
+    return (words_[s >> 6] >> (s & 63)) & 1;
+}
+
+long FilterSet::match_key(const uint8_t packed[32]) const {
+    if (!may_match(packed)) return -1;
+    const uint64_t head = head64(packed);
+    for (const Bucket& b : buckets_) {
+        const uint64_t probe = head & b.mask;
+        auto lo = std::lower_bound(b.keys.begin(), b.keys.end(), probe);
+        for (auto it = lo; it != b.keys.end() && *it == probe; ++it) {
+            const uint32_t owner = b.owners[(size_t)(it - b.keys.begin())];
+            if (filters_[owner].matches_key(packed)) return (long)owner;
+        }
+    }
+    return -1;
+}
+
+double FilterSet::match_probability() const {
+    double p = 0;
+    for (const PrefixFilter& f : filters_) p += std::pow(32.0, -(double)std::min(f.text.size(), KEY_ONLY_SYMBOLS));
+    return std::min(p, 1.0);
+}
+
+}  // namespace og

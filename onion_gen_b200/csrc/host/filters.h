@@ -1,0 +1,70 @@
+// Literal address-prefix filters and the prefix bitmap the device tests.
+//
+// Follows src/filter.rs for the prefix form: Filter::parse (bytes + mask of the
+// first min(len, 49) symbols, :649-685), FilterSet::new (sort, drop duplicates
+// and absorbed filters, :1326-1339), BitmapIndex (slot = top `bits` bits of the
+// packed key read big-endian, a prefix shorter than the index fills a run,
+// :2321-2604), the width choice (narrowest 16..24 at <= 1% occupancy, else the
+// widest that is <= 25% full, :2279-2295) and the exact match behind the bitmap
+// (length buckets with a binary search, :2645-2700). Wildcards, classes,
+// suffixes, substrings and regular expressions are not part of this engine.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace og {
+
+constexpr size_t KEY_ONLY_SYMBOLS = 49;
+constexpr size_t ADDRESS_SYMBOLS = 56;
+
+struct PrefixFilter {
+    std::string text;  // canonical: lowercase symbols
+    uint8_t bytes[32];
+    size_t nbytes;
+    uint8_t mask;
+    // filters longer than the key-only span need the full address checked
+    bool needs_full_check() const { return text.size() > KEY_ONLY_SYMBOLS; }
+    bool matches_key(const uint8_t packed[32]) const;
+};
+
+// Parses one filter; returns false and an explanation on error.
+bool parse_prefix(const std::string& raw, PrefixFilter& out, std::string& err);
+
+class FilterSet {
+public:
+    // bits == 0 chooses the width; otherwise 8..32.
+    bool build(std::vector<PrefixFilter> filters, uint32_t bits, std::string& err);
+
+    size_t size() const { return filters_.size(); }
+    const PrefixFilter& filter(size_t i) const { return filters_[i]; }
+    uint32_t bits() const { return bits_; }
+    const std::vector<uint64_t>& words() const { return words_; }
+    double occupancy() const;
+    bool may_match(const uint8_t packed[32]) const;
+    // index of the matching filter or -1; at most one matches because no kept
+    // filter is a prefix of another.
+    long match_key(const uint8_t packed[32]) const;
+    // expected fraction of candidates that match some filter exactly
+    double match_probability() const;
+
+private:
+    struct Bucket {
+        size_t symbols;
+        uint64_t mask;
+        std::vector<uint64_t> keys;
+        std::vector<uint32_t> owners;
+    };
+    std::vector<PrefixFilter> filters_;
+    std::vector<uint64_t> words_;
+    uint32_t bits_ = 0;
+    std::vector<Bucket> buckets_;
+};
+
+// Builds the bitmap over `filters` at `bits`; empty when more than a quarter
+// of the slots would be set.
+std::vector<uint64_t> build_bitmap(const std::vector<PrefixFilter>& filters, uint32_t bits);
+double bitmap_occupancy(const std::vector<uint64_t>& words, uint32_t bits);
+
+}  // namespace og

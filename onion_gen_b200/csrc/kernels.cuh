@@ -1,0 +1,107 @@
+// Device kernels of the key search and the host-side launch interface.
+//
+// Two enumeration schemes share one back end (Montgomery batch inversion,
+// canonical packing, prefix-bitmap test, warp-aggregated hit append):
+//
+//  * paired (the production engine). A lane holds an affine centre P. One
+//    round yields y(P + Q_m) and y(P - Q_m) for the table Q_m = 8m G,
+//    m = 1..half, plus y(P) itself, from the dedicated Edwards formulas
+//        y(P + Q) = (t1 - t2) / (x1 y2 - y1 x2),
+//        y(P - Q) = (t1 + t2) / (x1 y2 + y1 x2),      t = x y,
+//    i.e. two multiplications per pair, and moves P to the next centre
+//    P + W with x(P + W) = (t1 + tW) / (y1 yW - x1 xW) whose two divisions
+//    ride in the same batch. Every denominator of the round is inverted with
+//    one field inversion (Montgomery's trick, numerators folded into the
+//    forward products as in src/pairs.rs:174-224).
+//  * chain (the contract of src/batch.rs): a lane steps its projective point
+//    by +8G (seven multiplications, the addend's Z scaled to one) and
+//    batch-inverts Z over its `n` steps.
+//
+// Candidate numbering. Lane l of L in global round r ("window" w = r L + l):
+//   paired: index i in [0, 2 half] is the key of scalar offset
+//           8 (w (2 half + 1) + 1 + i); i = half is the centre, i = half + m
+//           is P + Q_m, i = half - m is P - Q_m.
+//   chain:  index t in [0, n) is the key of scalar offset 8 (w n + t).
+// Offsets never collide across lanes or rounds, and a run of R rounds covers
+// every candidate index of its range exactly once.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace og {
+
+// One bitmap survivor: 48 bytes, three 16-byte stores.
+struct HitRec {
+    uint32_t lane;
+    uint32_t step;  // round-in-launch * slots + candidate index
+    uint32_t search;
+    uint32_t pad;
+    uint32_t y[8];  // canonical y, little-endian limbs (the packed key, sign bit clear)
+};
+static_assert(sizeof(HitRec) == 48, "HitRec layout");
+
+struct FeWords {
+    uint32_t v[8];
+};
+
+struct PairedArgs {
+    const uint4* table;      // Q_m, m = 1..half: ((m-1)*3 + {x,y,t}) * 2 + q
+    uint4* lanes;            // affine centres: ({x,y} * 2 + q) * L + lane
+    uint4* scratch;          // ((e * 2 + {num,den}) * 2 + q) * L + lane, e < 2 half + 2
+    const uint32_t* bitmap;  // prefix bitmap as 32-bit words; nullptr = every candidate survives
+    uint32_t bits;
+    HitRec* hits;
+    uint32_t* counter;
+    uint32_t cap;
+    uint32_t search;         // copied into every record
+    FeWords wx, wy, wt;      // the round stride W = L (2 half + 1) 8 G, affine
+    uint32_t lanes_n;        // L, a multiple of the block size
+    uint32_t half;
+    uint32_t rounds;         // rounds per launch
+};
+
+struct ChainArgs {
+    uint4* lanes;            // projective points: ({X,Y,Z,T} * 2 + q) * L + lane
+    uint4* scratch;          // ((t * 2 + {num,den}) * 2 + q) * L + lane, t < n
+    const uint32_t* bitmap;
+    uint32_t bits;
+    HitRec* hits;
+    uint32_t* counter;
+    uint32_t cap;
+    uint32_t search;
+    FeWords step_ypx, step_ymx, step_t2d;  // +8G, Z = 1
+    FeWords jump_ypx, jump_ymx, jump_t2d;  // +8 (L-1) n G, Z = 1 (unused when L = 1)
+    uint32_t lanes_n;
+    uint32_t n;
+    uint32_t rounds;
+};
+
+// Lane start points: lane l starts at base + l * stride, built from the
+// binary expansion of l over `pow2` = { 2^k stride } in cached form with
+// Z = 1 (y+x, y-x, 2dxy). `affine_out` selects the paired layout (x, y)
+// over the chain layout (X, Y, Z, T).
+struct InitArgs {
+    uint4* lanes;
+    FeWords bx, by, bz, bt;  // base point, extended
+    const uint4* pow2;       // (k * 3 + {ypx,ymx,t2d}) * 2 + q
+    uint32_t nbits;
+    uint32_t lanes_n;
+    uint32_t affine_out;
+};
+
+cudaError_t launch_init(const InitArgs& a, int block, cudaStream_t s);
+cudaError_t launch_paired(const PairedArgs& a, int block, cudaStream_t s);
+cudaError_t launch_chain(const ChainArgs& a, int block, cudaStream_t s);
+
+// Register and shared-memory footprint of the search kernels, for the shape
+// choice.
+struct KernelInfo {
+    int regs;
+    int max_threads;
+    size_t local_bytes;
+    int blocks_per_sm;
+};
+cudaError_t paired_info(int block, uint32_t half, KernelInfo* info);
+cudaError_t chain_info(int block, KernelInfo* info);
+
+}  // namespace og

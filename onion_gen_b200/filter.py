@@ -1,0 +1,63 @@
+"""Literal-prefix filters (src/filter.rs), built by the engine's host code.
+
+``FilterSet.parse_all(["abc", "prefix:def"])`` sorts, drops absorbed filters,
+builds the prefix bitmap (width chosen as src/filter.rs:2279-2295 does unless
+``bits`` is given) and answers ``match_key`` exactly. Forms other than literal
+prefixes raise ``OgError`` (OG_E_FILTER).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+
+
+class FilterSet:
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def parse_all(cls, filters, bits: int = 0) -> "FilterSet":
+        text = "\n".join(filters).encode()
+        h = C.c_void_p()
+        err = N.errbuf()
+        N.check(N.lib.og_filters_new(text, bits, C.byref(h), err, 512), err)
+        return cls(h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            N.lib.og_filters_free(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __len__(self):
+        return N.lib.og_filters_count(self._h)
+
+    def texts(self):
+        out = []
+        b = C.create_string_buffer(64)
+        for i in range(len(self)):
+            N.lib.og_filters_text(self._h, i, b, 64)
+            out.append(b.value.decode())
+        return out
+
+    def index_words(self):
+        """(words uint64[], bits) — FilterSet::index_words (src/filter.rs:1857)."""
+        p = C.POINTER(C.c_uint64)()
+        n = N.lib.og_filters_words(self._h, C.byref(p))
+        return np.ctypeslib.as_array(p, shape=(n,)).copy(), N.lib.og_filters_bits(self._h)
+
+    @property
+    def bits(self) -> int:
+        return N.lib.og_filters_bits(self._h)
+
+    def occupancy(self) -> float:
+        return N.lib.og_filters_occupancy(self._h)
+
+    def match_key(self, packed: bytes):
+        """Index of the filter this packed key matches, or None."""
+        i = N.lib.og_filters_match(self._h, bytes(packed))
+        return None if i < 0 else i

@@ -1,0 +1,188 @@
+"""Parity of the sm_100a engine with the CPU oracle (runs on a B200: -m gpu).
+
+Every test drives the engine through the C ABI (libonion_gen_b200.so via
+ctypes) and checks it against the oracle's restatement of the reference
+engines on the same seeded inputs: bit-exact keys, exact offsets, exact
+survivor sets.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from onion_gen_b200 import _native as N
+from onion_gen_b200 import filter as F
+from onion_gen_b200 import gpu, key, workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def cfg(scheme, half, lanes, rounds, dump=1, block=128, room=0):
+    return N.EngineConfig(scheme, half, lanes, rounds, block, dump, room)
+
+
+def oracle_start(oracle, seed):
+    return oracle.scalar_base_mult(oracle.secret_scalar(seed))
+
+
+def sorted_run(engine, advances=1):
+    offs, keys = [], []
+    for _ in range(advances):
+        o, k = engine.advance_raw()
+        offs.append(o)
+        keys.append(k)
+    o = np.concatenate(offs)
+    k = np.concatenate(keys)
+    order = np.argsort(o, kind="stable")
+    return o[order], k[order]
+
+
+def test_chain_config1_bit_exact_against_batch_engine(oracle, device):
+    """4096 lanes x 256 steps, Z batch-inverted 256 at a time: all 2^20 keys
+    equal src/batch.rs's BatchEngine(256) from the same base scalar."""
+    start = oracle_start(oracle, workloads.seed(0))
+    eng = gpu.Engine(device, start, config=cfg(N.SCHEME_CHAIN, 256, 4096, 1))
+    assert eng.batch() == 1 << 20
+    offs, keys = sorted_run(eng)
+    assert np.array_equal(offs, 8 * np.arange(1 << 20, dtype=np.uint64))
+    want = np.frombuffer(oracle.chain_keys(start, 256, 1 << 20), dtype=np.uint8).reshape(-1, 32)
+    bad = np.nonzero((keys != want).any(axis=1))[0]
+    assert bad.size == 0, f"{bad.size} keys differ, first at offset {8 * int(bad[0])}"
+
+
+def test_paired_bit_exact_two_rounds(oracle, device):
+    start = oracle_start(oracle, workloads.seed(0))
+    eng = gpu.Engine(device, start, config=cfg(N.SCHEME_PAIRED, 128, 1024, 2))
+    n = 1024 * 257 * 2
+    assert eng.batch() == n
+    offs, keys = sorted_run(eng)
+    assert np.array_equal(offs, 8 * (1 + np.arange(n, dtype=np.uint64)))
+    want = np.frombuffer(oracle.chain_keys_mt(start, 1, n), dtype=np.uint8).reshape(-1, 32)
+    bad = np.nonzero((keys != want).any(axis=1))[0]
+    assert bad.size == 0, f"{bad.size} keys differ, first at offset {int(offs[bad[0]])}"
+
+
+@pytest.mark.parametrize("half,lanes,rounds", [(32, 256, 3), (1, 128, 2), (300, 384, 1)])
+def test_paired_consecutive_advances_tile_the_range(oracle, device, half, lanes, rounds):
+    """Two advances continue where the first stopped: no gap, no overlap."""
+    start = oracle_start(oracle, workloads.seed(7))
+    eng = gpu.Engine(device, start, config=cfg(N.SCHEME_PAIRED, half, lanes, rounds))
+    offs, keys = sorted_run(eng, advances=2)
+    n = 2 * lanes * (2 * half + 1) * rounds
+    assert np.array_equal(offs, 8 * (1 + np.arange(n, dtype=np.uint64)))
+    want = np.frombuffer(oracle.chain_keys_mt(start, 1, n), dtype=np.uint8).reshape(-1, 32)
+    assert np.array_equal(keys, want)
+
+
+def test_chain_two_advances_continue(oracle, device):
+    start = oracle_start(oracle, workloads.seed(3))
+    eng = gpu.Engine(device, start, config=cfg(N.SCHEME_CHAIN, 64, 256, 2))
+    offs, keys = sorted_run(eng, advances=2)
+    n = 2 * 256 * 64 * 2
+    assert np.array_equal(offs, 8 * np.arange(n, dtype=np.uint64))
+    want = np.frombuffer(oracle.chain_keys_mt(start, 0, n), dtype=np.uint8).reshape(-1, 32)
+    assert np.array_equal(keys, want)
+
+
+def test_reference_pair_engine_keys_appear_at_their_deltas(oracle, device):
+    """The reference's own paired CPU engine (src/pairs.rs) and this engine
+    agree on the key of every delta both produce."""
+    start = oracle_start(oracle, workloads.seed(11))
+    ref_keys, deltas = oracle.pair_keys(start, 96, 4)
+    ref = np.frombuffer(ref_keys, dtype=np.uint8).reshape(-1, 32)
+    eng = gpu.Engine(device, start, config=cfg(N.SCHEME_PAIRED, 96, 128, 1))
+    offs, keys = sorted_run(eng)
+    index = {int(o): i for i, o in enumerate(offs)}
+    for d, k in zip(deltas, ref):
+        assert np.array_equal(keys[index[int(d)]], k), f"delta {int(d)}"
+
+
+def filtered_parity(oracle, device, prefixes, bits, half, lanes, rounds, seed_i):
+    start = oracle_start(oracle, workloads.seed(seed_i))
+    fs = F.FilterSet.parse_all(prefixes, bits=bits)
+    words, b = fs.index_words()
+    ofs = oracle.FilterSet(prefixes, bits=bits)
+    assert b == ofs.bits and np.array_equal(words, ofs.words())
+    eng = gpu.Engine(device, start, bitmap=words, bitmap_bits=b, config=cfg(N.SCHEME_PAIRED, half, lanes, rounds, dump=0))
+    offs, keys = sorted_run(eng)
+    n = eng.batch()
+    # the oracle's survivors over the same range, in chunks
+    want = []
+    chunk = 1 << 22
+    for lo in range(0, n, chunk):
+        cnt = min(chunk, n - lo)
+        ks = np.frombuffer(oracle.chain_keys_mt(start, 1 + lo, cnt), dtype=np.uint8).reshape(-1, 32)
+        head = ks[:, :4].astype(np.uint32)
+        h32 = (head[:, 0] << 24) | (head[:, 1] << 16) | (head[:, 2] << 8) | head[:, 3]
+        slot = (h32 >> (32 - b)).astype(np.uint64)
+        hit = ((words[slot >> 6] >> (slot & 63)) & 1).astype(bool)
+        for i in np.nonzero(hit)[0]:
+            want.append((8 * (1 + lo + int(i)), bytes(ks[i])))
+    got = [(int(o), bytes(k)) for o, k in zip(offs, keys)]
+    assert got == want
+    return start, fs, got
+
+
+def test_paired_bitmap_survivors_equal_oracle(oracle, device):
+    """A 3-symbol prefix on a 16-bit index over 2^24 candidates: the exact
+    set of bitmap survivors, offsets and keys."""
+    start, fs, got = filtered_parity(oracle, device, ["abc"], 0, 128, 2048, 32, 1)
+    assert 300 < len(got) < 800  # 2^24 / 2^15 = 512 expected
+    seed = workloads.seed(1)
+    for off, packed in got:
+        pk, _ = key.check_hit(seed, off, packed)
+        assert pk[:31] == packed[:31]
+
+
+def test_paired_wide_bitmap_many_prefixes(oracle, device):
+    """Config 3's shape on a 2^22 sub-range: 10,000 prefixes of 3..8 symbols,
+    24-bit index at ~5% occupancy."""
+    prefixes = workloads.config3_prefixes()
+    start, fs, got = filtered_parity(oracle, device, prefixes, 0, 128, 1024, 16, 0)
+    assert fs.bits == 24
+    for off, packed in got[:200]:
+        key.check_hit(workloads.seed(0), off, packed)
+
+
+def test_overflow_is_an_error_not_a_truncation(oracle, device):
+    start = oracle_start(oracle, workloads.seed(0))
+    eng = gpu.Engine(device, start, config=cfg(N.SCHEME_PAIRED, 32, 128, 1, room=100))
+    with pytest.raises(N.OgError) as e:
+        eng.advance()
+    assert e.value.status == "OG_E_OVERFLOW"
+    with pytest.raises(N.OgError) as e:
+        eng.advance()
+    assert e.value.status == "OG_E_STATE"
+
+
+def test_reference_shaped_constructor_and_tuning_cache(oracle, device, tmp_path, monkeypatch):
+    """og_engine_new with threads=0 walks shapes, records the fastest in
+    tuning.yaml (format 1, the reference's key), and reuses it."""
+    path = tmp_path / "tuning.yaml"
+    monkeypatch.setenv("ONION_GEN_TUNING_FILE", str(path))
+    start = oracle_start(oracle, workloads.seed(0))
+    fs = F.FilterSet.parse_all([workloads.config2_prefix()])
+    words, bits = fs.index_words()
+    eng = gpu.Engine(device, start, threads=0, bitmap=words, bitmap_bits=bits)
+    text = path.read_text()
+    assert text.startswith("format: 1\nentries:\n")
+    assert f"device/{device.name}/cuda/0/" in text
+    shape = eng.shape()
+    eng2 = gpu.Engine(device, start, threads=0, bitmap=words, bitmap_bits=bits)
+    assert (eng2.shape().half, eng2.shape().lanes) == (shape.half, shape.lanes)
+    # survivors of the tuned engine are real keys
+    for s in eng2.advance()[:50]:
+        key.check_hit(workloads.seed(0), s.offset, s.packed)
+
+
+def test_threads_argument_is_lanes(oracle, device):
+    start = oracle_start(oracle, workloads.seed(0))
+    fs = F.FilterSet.parse_all(["ab"])
+    words, bits = fs.index_words()
+    eng = gpu.Engine(device, start, threads=1000, bitmap=words, bitmap_bits=bits)
+    assert eng.threads() == 1024  # rounded up to whole blocks
+    survivors = eng.advance()
+    assert survivors
+    for s in survivors[:100]:
+        key.check_hit(workloads.seed(0), s.offset, s.packed)
+        assert fs.match_key(s.packed) is not None

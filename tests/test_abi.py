@@ -1,0 +1,64 @@
+"""The C ABI library loads and exports every symbol include/*.h declares."""
+import ctypes
+import glob
+import os
+import re
+import subprocess
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(og_[a-z0-9_]+)\s*\(", text):
+            names.add(m.group(1))
+    return names
+
+
+def test_every_declared_symbol_is_exported(native):
+    lib = ctypes.CDLL(native._native.LIB_PATH)
+    names = declared_functions()
+    assert len(names) > 25
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_exports_are_only_the_c_abi(native):
+    out = subprocess.run(["nm", "-D", "--defined-only", native._native.LIB_PATH], capture_output=True, text=True).stdout
+    exported = {l.split()[-1] for l in out.splitlines() if " T " in l and l.split()[-1].startswith("og_")}
+    assert exported == declared_functions()
+
+
+def test_no_device_is_an_ordinary_outcome(native):
+    """cuda::look (src/gpu/cuda.rs:35-77): no device is a status, not a crash."""
+    n = ctypes.c_int(-1)
+    err = native._native.errbuf()
+    rc = native._native.lib.og_device_count(ctypes.byref(n), err, 512)
+    if rc == 0:
+        assert n.value >= 1
+    else:
+        assert native._native.STATUS[rc] == "OG_E_NODEVICE"
+        assert n.value == 0
+        assert native.gpu.look() == []
+
+
+def test_engine_without_device_reports_status(native, oracle):
+    import pytest
+
+    if native.gpu.look():
+        pytest.skip("a device is present; covered by the gpu tests")
+    start = oracle.scalar_base_mult(oracle.secret_scalar(bytes(32)))
+    with pytest.raises(native._native.OgError) as e:
+        native.gpu.Engine(0, start, threads=128, bitmap=[0] * 1024, bitmap_bits=16)
+    assert e.value.status == "OG_E_NODEVICE"
+
+
+def test_product_does_not_reference_the_oracle():
+    """The product (package and C++/CUDA sources) never imports or loads the oracle."""
+    pat = re.compile(r"(from|import)\s+oracle\b|liboracle|oracle/")
+    for path in glob.glob(os.path.join(ROOT, "onion_gen_b200", "**", "*"), recursive=True):
+        if os.path.isfile(path) and path.endswith((".py", ".cu", ".cuh", ".cpp", ".h")):
+            assert not pat.search(open(path, errors="replace").read()), path

@@ -39,7 +39,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 CANDIDATES_PER_STEP = 1 << 32
-HALF = 128
+HALF = 256
 CPU_HALF = 4096  # PairEngine::new(8192) (src/run.rs:601, src/batch.rs:32)
 
 
@@ -51,6 +51,9 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--case", default="full", choices=["full", "small"],
+                   help="small: the profiling case, three one-round advances of the plain engine")
+    p.add_argument("--half", type=int, default=HALF)
     return p.parse_args()
 
 
@@ -191,10 +194,31 @@ def pp_per_candidate(half):
     return ((21 + 10 * half) * 64 + 254 * 36) / (2 * half + 1)
 
 
+def small_case(args):
+    """Three advances of one round each at the default shape: the case the
+    ncu summaries under profiles/ are captured on (about 1.6 GB of scratch)."""
+    from onion_gen_b200 import _native as N
+    from onion_gen_b200 import filter as F
+    from onion_gen_b200 import gpu, key, workloads
+
+    dev = gpu.look()[0]
+    fs = F.FilterSet.parse_all([workloads.config2_prefix()])
+    words, bits = fs.index_words()
+    start = key.start_point(workloads.seed(0))
+    eng = gpu.Engine(dev, start, bitmap=words, bitmap_bits=bits, config=N.EngineConfig(0, args.half, 0, 1, 128, 0, 0))
+    for i in range(3):
+        o, _ = eng.advance_raw()
+        ms = eng.last_kernel_ms()
+        print(f"advance {i}: {len(o)} survivors, kernel {ms:.3f} ms, {eng.batch() / ms * 1e3:.4e} keys/s")
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         reference_arm(args)
+        return
+    if args.case == "small":
+        small_case(args)
         return
     rank, world, local = dist_env()
     import ctypes as C
@@ -231,7 +255,7 @@ def main():
     scalar = int.from_bytes(key.secret_scalar(seed), "little") + (rank << 43)
     base = key.scalar_base_mult(scalar.to_bytes(32, "little"))
 
-    cfg = N.EngineConfig(N.SCHEME_PAIRED, HALF, 0, 0, 128, 0, 0)
+    cfg = N.EngineConfig(N.SCHEME_PAIRED, args.half, 0, 0, 128, 0, 0)
     eng = gpu.Engine(dev, base, bitmap=words, bitmap_bits=bits, config=cfg)
     shape = eng.shape()
     batch = eng.batch()

@@ -9,7 +9,7 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libonion_gen_b200.so")
+LIB_PATH = os.environ.get("ONION_GEN_B200_LIB") or os.path.join(HERE, "libonion_gen_b200.so")
 
 OG_OK = 0
 STATUS = {

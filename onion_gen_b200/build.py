@@ -46,8 +46,8 @@ def _stale(obj, src, hdr_mtime):
     return t < os.path.getmtime(src) or t < hdr_mtime
 
 
-def _compile(src, obj, is_cu, verbose):
-    cmd = [NVCC] + COMMON
+def _compile(src, obj, is_cu, verbose, extra=()):
+    cmd = [NVCC] + COMMON + list(extra)
     if is_cu:
         cmd += ARCH + ["-lineinfo", "-Xptxas", "-v"] if verbose else ARCH + ["-lineinfo"]
     else:
@@ -59,26 +59,29 @@ def _compile(src, obj, is_cu, verbose):
     return r.stderr
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    os.makedirs(OUT, exist_ok=True)
+def build(force: bool = False, verbose: bool = False, extra=(), lib=None, out=None) -> str:
+    """Builds the library (``lib``, objects in ``out``) with optional extra nvcc flags."""
+    lib = lib or LIB
+    out = out or OUT
+    os.makedirs(out, exist_ok=True)
     cu, cpp = sources()
     hdr = max((os.path.getmtime(h) for h in headers()), default=0)
     jobs = []
     objs = []
     for src in cu + cpp:
         rel = os.path.relpath(src, CSRC).replace(os.sep, "_")
-        obj = os.path.join(OUT, rel + ".o")
+        obj = os.path.join(out, rel + ".o")
         objs.append(obj)
         if force or _stale(obj, src, hdr):
             jobs.append((src, obj, src.endswith(".cu")))
     logs = []
     if jobs:
         with cf.ThreadPoolExecutor(max_workers=min(8, len(jobs))) as ex:
-            futs = [ex.submit(_compile, s, o, c, verbose) for s, o, c in jobs]
+            futs = [ex.submit(_compile, s, o, c, verbose, extra) for s, o, c in jobs]
             for f in futs:
                 logs.append(f.result())
-    if jobs or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lpthread"]
+    if jobs or not os.path.exists(lib) or any(os.path.getmtime(o) > os.path.getmtime(lib) for o in objs):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", lib] + objs + ["-lcudart", "-lpthread"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
@@ -86,7 +89,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         for l in logs:
             if l:
                 print(l)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":

@@ -22,6 +22,10 @@
 #include "host/tuning.h"
 #include "kernels.cuh"
 
+#ifndef OG_LB_THREADS
+#define OG_LB_THREADS 128
+#endif
+
 using namespace og;
 
 namespace og {
@@ -177,13 +181,17 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
     }
     CU(cudaSetDevice(ordinal));
     if (cfg.block == 0) cfg.block = 128;
-    if (cfg.block % 32 || cfg.block > 256) return fail(err, errlen, OG_E_ARG, "block %u (a multiple of 32, at most 256)", cfg.block);
-    if (cfg.half == 0) cfg.half = cfg.scheme == OG_SCHEME_CHAIN ? 256 : 128;
+    if (cfg.block % 32 || cfg.block > OG_LB_THREADS)
+        return fail(err, errlen, OG_E_ARG, "block %u (a multiple of 32, at most %d)", cfg.block, OG_LB_THREADS);
+    if (cfg.half == 0) cfg.half = 256;
     if (cfg.scheme == OG_SCHEME_PAIRED && cfg.half > 2048) return fail(err, errlen, OG_E_ARG, "half %u > 2048", cfg.half);
     if (cfg.scheme == OG_SCHEME_CHAIN && cfg.half > 65536) return fail(err, errlen, OG_E_ARG, "n %u > 65536", cfg.half);
     if (cfg.lanes == 0) {
+        // two waves of resident blocks: measured 5% ahead of one, as the
+        // second wave overlaps the first's tail
         int rc = resident_lanes(ordinal, cfg.scheme, cfg.half, cfg.block, &cfg.lanes, err, errlen);
         if (rc) return rc;
+        cfg.lanes *= 2;
     }
     cfg.lanes = (cfg.lanes + cfg.block - 1) / cfg.block * cfg.block;
     if (cfg.lanes > (1u << 24)) return fail(err, errlen, OG_E_ARG, "%u lanes (at most 2^24)", cfg.lanes);
@@ -379,10 +387,10 @@ int og_engine_new(int ordinal, const uint8_t start[128], uint32_t threads, const
     og_engine* best = nullptr;
     double best_rate = -1;
     int last = OG_E_DEVICE;
-    for (uint32_t half : {64u, 128u, 256u}) {
+    for (uint32_t half : {128u, 256u, 512u}) {
         uint32_t resident = 0;
         if (resident_lanes(ordinal, OG_SCHEME_PAIRED, half, 128, &resident, err, errlen) != OG_OK) continue;
-        for (uint32_t mult : {1u, 2u, 4u}) {
+        for (uint32_t mult : {1u, 2u, 3u}) {
             og_engine_config c{};
             c.scheme = OG_SCHEME_PAIRED;
             c.half = half;

@@ -18,12 +18,14 @@ struct fe {
     uint32_t v[8];
 };
 
-__device__ __forceinline__ void fe_mul(fe& r, const fe& a, const fe& b) { fe_mul_asm(r.v, a.v, b.v); }
+#define OG_FE_MUL_ASM fe_mul_asm
+
+__device__ __forceinline__ void fe_mul(fe& r, const fe& a, const fe& b) { OG_FE_MUL_ASM(r.v, a.v, b.v); }
 __device__ __forceinline__ void fe_sq(fe& r, const fe& a) { fe_sq_asm(r.v, a.v); }
 
 __device__ __forceinline__ fe fe_mulv(const fe& a, const fe& b) {
     fe r;
-    fe_mul_asm(r.v, a.v, b.v);
+    OG_FE_MUL_ASM(r.v, a.v, b.v);
     return r;
 }
 

@@ -1,113 +1,139 @@
 """Generates field_asm.cuh: GF(2^255-19) multiply and square for sm_100a.
 
-Eight 32-bit limbs, least significant first, values below 2^256 (not
-canonical). The 512-bit product is built row by row with two PTX carry
-chains per row (low halves, then high halves), and folded with
-2^256 = 38 (mod 2^255-19). Each routine is one asm block so the carry flag
-never crosses a compiler-visible boundary.
+Eight 32-bit limbs, least significant first; inputs and outputs below 2^256
+(not canonical). The 512-bit product is accumulated by product scanning in
+64-bit slots: every partial product a_i*b_j is added as one 64-bit quantity
+(its low half then its high half, back to back in one PTX carry chain), so
+the pair maps to one wide multiply-add. Row i runs two chains: products whose
+position i+j is even (slots (i,i+1), (i+2,i+3), ...), then the odd ones. The
+accumulated value after each chain is below 2^(32*(i+9)), which is what lets
+the carry out of word i+8 be dropped and a fresh word take a bare carry.
+The 512-bit result is folded with 2^256 = 38 (mod 2^255-19) the same way.
+(A one-level Karatsuba variant, 48 wide products plus carry corrections on
+the ALU, measured no faster on sm_100a: the ALU work it adds cancels the
+multiply-pipe work it saves.)
 
-Run: python gen_field_asm.py > field_asm.cuh
+Each routine is one asm block so the carry flag never crosses a
+compiler-visible boundary.
+
+    python gen_field_asm.py > field_asm.cuh       # write the header
+    python gen_field_asm.py --check               # simulate the PTX on random inputs
 """
+import random
+import sys
 
 
-def mul_body():
-    L = []
-    A = lambda i: f"%{8 + i}"
-    B = lambda j: f"%{16 + j}"
-    T = lambda k: f"t{k}"
-    # row 0: low halves straight into t0..t7, high halves into t1..t8
-    for j in range(8):
-        L.append(f"mul.lo.u32 {T(j)}, {A(0)}, {B(j)};")
-    for j in range(8):
-        op = "mad.hi.cc.u32" if j == 0 else ("madc.hi.u32" if j == 7 else "madc.hi.cc.u32")
-        acc = "0" if j == 7 else T(j + 1)
-        L.append(f"{op} {T(j + 1)}, {A(0)}, {B(j)}, {acc};")
-    for i in range(1, 8):
-        for j in range(8):
-            op = "mad.lo.cc.u32" if j == 0 else "madc.lo.cc.u32"
-            L.append(f"{op} {T(i + j)}, {A(i)}, {B(j)}, {T(i + j)};")
-        L.append(f"addc.u32 {T(i + 8)}, 0, 0;")
-        for j in range(8):
-            op = "mad.hi.cc.u32" if j == 0 else ("madc.hi.u32" if j == 7 else "madc.hi.cc.u32")
-            L.append(f"{op} {T(i + j + 1)}, {A(i)}, {B(j)}, {T(i + j + 1)};")
-    return L
+class Emit:
+    """Accumulates PTX lines and tracks which accumulator words hold data."""
+
+    def __init__(self, acc="t", words=17):
+        self.lines = []
+        self.acc = acc
+        self.live = [False] * words
+
+    def w(self, k):
+        return f"{self.acc}{k}"
+
+    def chain(self, prods, carry_to=None):
+        """prods: list of (position, x, y); positions ascend by 2 so the 64-bit
+        slots do not overlap. Adds every x*y at its position in one carry
+        chain; the final carry goes to `carry_to` when given (a word that
+        may be fresh), else is known to be zero."""
+        ops = []
+        for n, (p, x, y) in enumerate(prods):
+            for half, q in (("lo", p), ("hi", p + 1)):
+                ops.append((half, q, x, y))
+        for n, (half, q, x, y) in enumerate(ops):
+            first, last = n == 0, n == len(ops) - 1
+            cc_in = not first
+            cc_out = not last or carry_to is not None
+            addend = self.w(q) if self.live[q] else "0"
+            op = ("madc" if cc_in else "mad") + f".{half}" + (".cc" if cc_out else "") + ".u32"
+            self.lines.append(f"{op} {self.w(q)}, {x}, {y}, {addend};")
+            self.live[q] = True
+        if carry_to is not None:
+            src = self.w(carry_to) if self.live[carry_to] else "0"
+            self.lines.append(f"addc.u32 {self.w(carry_to)}, {src}, 0;")
+            self.live[carry_to] = True
 
 
-def sq_body():
-    L = []
-    A = lambda i: f"%{8 + i}"
-    T = lambda k: f"t{k}"
-    # off-diagonal products a_i a_j, i < j: low half to t[i+j], high to t[i+j+1]
-    for j in range(1, 8):
-        L.append(f"mul.lo.u32 {T(j)}, {A(0)}, {A(j)};")
-    for j in range(1, 8):
-        first, last = j == 1, j == 7
-        op = "mad.hi.cc.u32" if first else ("madc.hi.u32" if last else "madc.hi.cc.u32")
-        acc = "0" if last else T(j + 1)
-        L.append(f"{op} {T(j + 1)}, {A(0)}, {A(j)}, {acc};")
-    for i in range(1, 7):
+def mul_body(A, Bv):
+    e = Emit("t")
+    for i in range(8):
+        even = [(i + j, A(i), Bv(j)) for j in range(0, 8, 2)]
+        odd = [(i + j, A(i), Bv(j)) for j in range(1, 8, 2)]
+        e.chain(even, carry_to=i + 8)
+        e.chain(odd, carry_to=None)
+    return e.lines
+
+
+def sq_body(A):
+    e = Emit("t")
+    # off-diagonal products a_i a_j, i < j, at position i + j
+    for i in range(7):
         js = list(range(i + 1, 8))
-        for n, j in enumerate(js):
-            op = "mad.lo.cc.u32" if n == 0 else "madc.lo.cc.u32"
-            L.append(f"{op} {T(i + j)}, {A(i)}, {A(j)}, {T(i + j)};")
-        L.append(f"addc.u32 {T(i + 8)}, 0, 0;")
-        for n, j in enumerate(js):
-            first, last = n == 0, n == len(js) - 1
-            if first and last:
-                op = "mad.hi.u32"
-            elif first:
-                op = "mad.hi.cc.u32"
-            elif last:
-                op = "madc.hi.u32"
-            else:
-                op = "madc.hi.cc.u32"
-            L.append(f"{op} {T(i + j + 1)}, {A(i)}, {A(j)}, {T(i + j + 1)};")
-    # double t1..t14 into t1..t15
+        even = [(i + j, A(i), A(j)) for j in js if (j - (i + 1)) % 2 == 0]
+        odd = [(i + j, A(i), A(j)) for j in js if (j - (i + 1)) % 2 == 1]
+        top = i + 8 if i + 8 <= 15 else None
+        if even:
+            last_even_hi = even[-1][0] + 1
+            e.chain(even, carry_to=last_even_hi + 1 if last_even_hi + 1 <= 15 else None)
+        if odd:
+            last_odd_hi = odd[-1][0] + 1
+            e.chain(odd, carry_to=last_odd_hi + 1 if last_odd_hi + 1 <= 15 else None)
+    L = e.lines
+    # double t1..t14 (t0 is still empty), carry into t15
+    for k in range(16):
+        if not e.live[k]:
+            L.append(f"mov.u32 t{k}, 0;")
+            e.live[k] = True
     L.append("add.cc.u32 t1, t1, t1;")
     for k in range(2, 15):
-        L.append(f"addc.cc.u32 {T(k)}, {T(k)}, {T(k)};")
-    L.append("addc.u32 t15, 0, 0;")
-    # diagonal squares
-    L.append(f"mul.lo.u32 t0, {A(0)}, {A(0)};")
-    L.append(f"mad.hi.cc.u32 t1, {A(0)}, {A(0)}, t1;")
-    for i in range(1, 8):
-        L.append(f"madc.lo.cc.u32 {T(2 * i)}, {A(i)}, {A(i)}, {T(2 * i)};")
-        op = "madc.hi.u32" if i == 7 else "madc.hi.cc.u32"
-        L.append(f"{op} {T(2 * i + 1)}, {A(i)}, {A(i)}, {T(2 * i + 1)};")
+        L.append(f"addc.cc.u32 t{k}, t{k}, t{k};")
+    L.append("addc.u32 t15, t15, t15;")
+    # diagonal squares a_i^2 at position 2i: one chain of 64-bit slots
+    diag = [(2 * i, A(i), A(i)) for i in range(8)]
+    e.chain(diag, carry_to=None)
     return L
 
 
 def reduce_tail():
-    """t0..t15 -> %0..%7 with 2^256 = 38, result below 2^256."""
-    R = lambda k: f"%{k}"
-    T = lambda k: f"t{k}"
+    """t0..t15 -> %0..%7 with 2^256 = 38; the result is below 2^256."""
+    e = Emit("r")
     L = []
+    # r = t_lo, then r += 38 * t_hi by two chains of 64-bit slots
     for k in range(8):
-        op = "mad.lo.cc.u32" if k == 0 else "madc.lo.cc.u32"
-        L.append(f"{op} {R(k)}, {T(8 + k)}, 38, {T(k)};")
-    L.append("addc.u32 c, 0, 0;")
-    for k in range(8):
-        op = "mad.hi.cc.u32" if k == 0 else ("madc.hi.u32" if k == 7 else "madc.hi.cc.u32")
-        dst = "c" if k == 7 else R(k + 1)
-        L.append(f"{op} {dst}, {T(8 + k)}, 38, {dst};")
-    # value = %0..%7 + c * 2^256 with c < 39: fold once more
-    L.append("mad.lo.cc.u32 %0, c, 38, %0;")
+        L.append(f"mov.u32 r{k}, t{k};")
+        e.live[k] = True
+    even = [(k, f"t{8 + k}", "38") for k in range(0, 8, 2)]
+    odd = [(k, f"t{8 + k}", "38") for k in range(1, 8, 2)]
+    e.chain(even, carry_to=8)
+    e.chain(odd, carry_to=None)
+    L += e.lines
+    # value = r0..r7 + r8 * 2^256 with r8 < 39: fold once more
+    L.append("mad.lo.cc.u32 r0, r8, 38, r0;")
     for k in range(1, 8):
-        L.append(f"addc.cc.u32 {R(k)}, {R(k)}, 0;")
-    L.append("addc.u32 c, 0, 0;")
-    # a carry here leaves %0..%7 below 38*39, so this add cannot carry
-    L.append("mad.lo.u32 %0, c, 38, %0;")
+        L.append(f"addc.cc.u32 r{k}, r{k}, 0;")
+    L.append("addc.u32 r8, 0, 0;")
+    # a carry here leaves r0..r7 below 38*39, so this add cannot carry
+    L.append("mad.lo.u32 r0, r8, 38, r0;")
+    for k in range(8):
+        L.append(f"mov.u32 %{k}, r{k};")
     return L
 
 
-def emit(name, body, nin):
+def emit_fn(name, body, nin, extra=""):
     out = []
     ins = ", ".join(f'"r"(a[{i}])' for i in range(8))
     if nin == 2:
         ins += ", " + ", ".join(f'"r"(b[{i}])' for i in range(8))
-    sig = "const uint32_t* __restrict__ a, const uint32_t* __restrict__ b" if nin == 2 else "const uint32_t* __restrict__ a"
+    sig = (
+        "const uint32_t* __restrict__ a, const uint32_t* __restrict__ b"
+        if nin == 2
+        else "const uint32_t* __restrict__ a"
+    )
     out.append(f"__device__ __forceinline__ void {name}(uint32_t* __restrict__ r, {sig}) {{")
-    out.append("    asm(\"{\\n\\t.reg .u32 t<16>;\\n\\t.reg .u32 c;\\n\\t\"")
+    out.append('    asm("{\\n\\t.reg .u32 t<17>;\\n\\t.reg .u32 r<9>;\\n\\t' + extra + '"')
     for line in body + reduce_tail():
         out.append(f'        "{line}\\n\\t"')
     out.append('        "}"')
@@ -118,12 +144,131 @@ def emit(name, body, nin):
     return "\n".join(out)
 
 
+def operands():
+    A = lambda i: f"%{8 + i}"
+    Bv = lambda j: f"%{16 + j}"
+    return A, Bv
+
+
+def header():
+    A, Bv = operands()
+    parts = [
+        "// Generated by gen_field_asm.py — do not edit by hand.",
+        "// GF(2^255-19): r = a*b and r = a^2, eight 32-bit limbs, result below 2^256.",
+        "#pragma once",
+        "#include <cstdint>",
+        "",
+        emit_fn("fe_mul_asm", mul_body(A, Bv), 2),
+        "",
+        emit_fn("fe_sq_asm", sq_body(A), 1),
+        "",
+
+    ]
+    return "\n".join(parts)
+
+
+# ---- a small interpreter of the PTX subset above, for --check ----------------
+
+M32 = (1 << 32) - 1
+
+
+def simulate(lines, args):
+    regs = {}
+    cc = 0
+
+    def val(x):
+        if x.startswith("%"):
+            return args[int(x[1:])]
+        if x[0].isdigit():
+            return int(x)
+        return regs[x]
+
+    out = {}
+    for line in lines:
+        line = line.rstrip(";")
+        op, rest = line.split(" ", 1)
+        ops = [s.strip() for s in rest.split(",")]
+        parts = op.split(".")
+        base = parts[0]
+        dst = ops[0]
+        if base in ("mad", "madc", "mul"):
+            half = parts[1]
+            x, y = val(ops[1]), val(ops[2])
+            prod = x * y
+            v = (prod & M32) if half == "lo" else (prod >> 32)
+            if base == "mul":
+                res = v
+                carry = 0
+            else:
+                add = val(ops[3])
+                cin = cc if base == "madc" else 0
+                s = v + add + cin
+                res, carry = s & M32, s >> 32
+            if ".cc" in op:
+                cc = carry
+            elif base != "mul" and carry:
+                raise AssertionError(f"carry lost in {line}")
+        elif base in ("add", "addc"):
+            s = val(ops[1]) + val(ops[2]) + (cc if base == "addc" else 0)
+            res, carry = s & M32, s >> 32
+            if ".cc" in op:
+                cc = carry
+            elif carry:
+                raise AssertionError(f"carry lost in {line}")
+        elif base == "mov":
+            res = val(ops[1])
+        elif base == "neg":
+            res = (-val(ops[1])) & M32
+        elif base == "and":
+            res = val(ops[1]) & val(ops[2])
+        elif base in ("sub", "subc"):
+            d = val(ops[1]) - val(ops[2]) - (cc if base == "subc" else 0)
+            res, borrow = d & M32, 1 if d < 0 else 0
+            if ".cc" in op:
+                cc = borrow
+            elif borrow:
+                raise AssertionError(f"borrow lost in {line}")
+        else:
+            raise ValueError(op)
+        if dst.startswith("%"):
+            out[int(dst[1:])] = res
+        else:
+            regs[dst] = res
+    return [out[k] for k in range(8)]
+
+
+def limbs(v):
+    return [(v >> (32 * k)) & M32 for k in range(8)]
+
+
+def check(n=20000):
+    P = 2**255 - 19
+    A, Bv = operands()
+    mul = mul_body(A, Bv) + reduce_tail()
+    sq = sq_body(A) + reduce_tail()
+
+    rng = random.Random(1)
+    special = [0, 1, 2**256 - 1, 2**255, 2**256 - 38, P, 2 * P, 2**255 - 1, 38]
+    vals = special + [rng.getrandbits(256) for _ in range(n)]
+    for i, a in enumerate(vals):
+        b = vals[(i * 13 + 7) % len(vals)] if i % 3 else rng.getrandbits(256)
+        r = simulate(mul, {**{8 + k: v for k, v in enumerate(limbs(a))}, **{16 + k: v for k, v in enumerate(limbs(b))}})
+        rv = sum(x << (32 * k) for k, x in enumerate(r))
+        assert rv < 2**256 and rv % P == a * b % P, (hex(a), hex(b))
+        r = simulate(sq, {8 + k: v for k, v in enumerate(limbs(a))})
+        rv = sum(x << (32 * k) for k, x in enumerate(r))
+        assert rv < 2**256 and rv % P == a * a % P, hex(a)
+    # extremes that stress every carry: all-ones limbs
+    for a in [2**256 - 1, 2**256 - 2, (2**256 - 1) ^ (1 << 200)]:
+        for b in [2**256 - 1, 2**255 + 12345]:
+            r = simulate(mul, {**{8 + k: v for k, v in enumerate(limbs(a))}, **{16 + k: v for k, v in enumerate(limbs(b))}})
+            rv = sum(x << (32 * k) for k, x in enumerate(r))
+            assert rv % P == a * b % P
+    print(f"ok: {len(vals)} multiplications and squarings; mul {len(mul)} ops, sq {len(sq)} ops")
+
+
 if __name__ == "__main__":
-    print("// Generated by gen_field_asm.py — do not edit by hand.")
-    print("// GF(2^255-19): r = a*b and r = a^2, eight 32-bit limbs, result below 2^256.")
-    print("#pragma once")
-    print("#include <cstdint>")
-    print()
-    print(emit("fe_mul_asm", mul_body(), 2))
-    print()
-    print(emit("fe_sq_asm", sq_body(), 1))
+    if "--check" in sys.argv:
+        check()
+    else:
+        print(header())

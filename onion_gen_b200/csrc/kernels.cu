@@ -3,6 +3,17 @@
 #include "field.cuh"
 #include "kernels.cuh"
 
+// Register budget of the search kernels: at most OG_LB_THREADS threads per
+// block and at least OG_LB_MIN_BLOCKS resident blocks per SM. 128 x 6 caps
+// them at 80 registers (24 warps per SM), measured fastest on B200 against
+// 96 (20 warps), 128 (16) and 130 registers.
+#ifndef OG_LB_THREADS
+#define OG_LB_THREADS 128
+#endif
+#ifndef OG_LB_MIN_BLOCKS
+#define OG_LB_MIN_BLOCKS 6
+#endif
+
 namespace og {
 
 namespace {
@@ -110,7 +121,7 @@ __global__ void __launch_bounds__(128) init_kernel(const InitArgs a) {
     }
 }
 
-__global__ void __launch_bounds__(256) paired_kernel(const PairedArgs a) {
+__global__ void __launch_bounds__(OG_LB_THREADS, OG_LB_MIN_BLOCKS) paired_kernel(const PairedArgs a) {
     extern __shared__ uint4 qtab[];
     for (uint32_t i = threadIdx.x; i < a.half * 6; i += blockDim.x) qtab[i] = a.table[i];
     __syncthreads();
@@ -181,7 +192,8 @@ __global__ void __launch_bounds__(256) paired_kernel(const PairedArgs a) {
     store_fe(a.lanes + 2 * L + lane, L, y);
 }
 
-__global__ void __launch_bounds__(256) chain_kernel(const ChainArgs a) {
+// the chain kernel (parity contract, not the production path) keeps 96 registers: at 80 it spills
+__global__ void __launch_bounds__(OG_LB_THREADS, 5) chain_kernel(const ChainArgs a) {
     const uint32_t lane = blockIdx.x * blockDim.x + threadIdx.x;
     const size_t L = a.lanes_n;
     const Sink sink{a.bitmap, a.bits, a.hits, a.counter, a.cap, a.search};

@@ -115,6 +115,80 @@ float og_engine_last_kernel_ms(const og_engine* e);
 
 void og_engine_free(og_engine* e);
 
+/* ---- the batched engine: many searches in one persistent kernel ---------
+ *
+ * No counterpart in the reference (its device engine runs one search per
+ * device thread, src/run.rs:1030-1119). Every search is a seeded base scalar
+ * (key::secret_scalar, src/key.rs:23-29), a literal-prefix filter set and a
+ * quota. All admitted searches advance together: one step replays a captured
+ * CUDA graph that runs one persistent kernel over every search's lanes, then
+ * matches the bitmap survivors exactly on the device. Every exact hit is
+ * re-derived and verified on the host before it counts (src/run.rs:1089-1111).
+ *
+ * A search's result is its first `quota` hits in offset order. Offsets are a
+ * pure function of the search (candidate windows are processed in contiguous
+ * increasing order whatever the lanes it holds), so the result is the same
+ * whether the search runs alone or beside any others. */
+
+typedef struct og_batch og_batch;
+
+typedef struct og_batch_config {
+    uint32_t half;          /* table size of every search; a round is 2*half+1 keys (0: 256) */
+    uint32_t slots;         /* lanes in the shared pool, a multiple of 128 (0: two waves of resident blocks) */
+    uint32_t rounds;        /* rounds per step (0: 1) */
+    uint32_t max_searches;  /* searches admitted at once (0: 4096) */
+    uint32_t max_hits;      /* exact hits one step may return (0: 65536) */
+    uint32_t graph;         /* 0 or 1: replay each step as a captured CUDA graph; 2: plain launches */
+    uint64_t memory_budget; /* device bytes for per-search tables (0: half of the free memory after the pool) */
+} og_batch_config;
+
+typedef struct og_batch_hit {
+    uint64_t search_id;
+    uint64_t offset;     /* scalar delta from the search's base scalar */
+    uint8_t packed[32];  /* the public key, sign bit clear */
+    uint8_t public_key[32]; /* the full public key (sign set), as re-derived on the host */
+    uint32_t filter;     /* index of the matching filter in the search's sorted set */
+    uint32_t pad;
+} og_batch_hit;
+
+typedef struct og_search_status {
+    uint64_t windows;    /* candidate windows fully processed */
+    uint64_t candidates; /* = windows * (2*half+1) */
+    uint64_t hits;       /* verified hits found so far */
+    uint32_t lanes;      /* lanes held in the last step */
+    uint32_t quota;
+    uint32_t done;       /* 1 once the first `quota` hits are known */
+    uint32_t filters;
+    uint64_t table_bytes;/* device bytes of its bitmap and exact-match tables */
+} og_search_status;
+
+int og_batch_new(int ordinal, const og_batch_config* cfg, og_batch** out, char* err, size_t errlen);
+/* Admits a search: `filters` newline-separated literal prefixes. Fails with
+ * OG_E_NOMEM when its tables do not fit the memory budget (nothing is
+ * changed), OG_E_CAPACITY when max_searches are admitted. */
+int og_batch_admit(og_batch* b, uint64_t search_id, const uint8_t seed[32], const char* filters, uint32_t quota,
+                   char* err, size_t errlen);
+/* One step: every admitted, unfinished search advances `rounds` rounds.
+ * Writes this step's verified hits to `out` (room `cap`, og_batch_room()). */
+int og_batch_step(og_batch* b, og_batch_hit* out, size_t cap, size_t* n, char* err, size_t errlen);
+size_t og_batch_room(const og_batch* b);
+int og_batch_status(const og_batch* b, uint64_t search_id, og_search_status* st);
+/* The result of a finished search: its first `quota` hits in offset order. */
+int og_batch_results(const og_batch* b, uint64_t search_id, og_batch_hit* out, size_t cap, size_t* n);
+/* Removes a search (finished or not) and frees its lanes and tables. */
+int og_batch_retire(og_batch* b, uint64_t search_id);
+/* Searches admitted and not yet retired; of them, unfinished. */
+void og_batch_counts(const og_batch* b, size_t* admitted, size_t* running);
+/* Device time of the last step (CUDA events around the graph), ms. */
+float og_batch_last_step_ms(const og_batch* b);
+/* Candidates examined in the last step, all searches. */
+uint64_t og_batch_last_step_candidates(const og_batch* b);
+/* Kernel launches the last step made (graph nodes that are kernels). */
+uint32_t og_batch_last_step_launches(const og_batch* b);
+/* Device bytes of per-search tables in use, and the budget. */
+void og_batch_memory(const og_batch* b, uint64_t* used, uint64_t* budget);
+void og_batch_free(og_batch* b);
+
 /* ---- measurement --------------------------------------------------------- */
 
 /* The integer-multiply roofline of device `ordinal`, measured: the issue

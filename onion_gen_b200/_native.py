@@ -54,6 +54,42 @@ class EngineConfig(C.Structure):
     ]
 
 
+class BatchConfig(C.Structure):
+    _fields_ = [
+        ("half", C.c_uint32),
+        ("slots", C.c_uint32),
+        ("rounds", C.c_uint32),
+        ("max_searches", C.c_uint32),
+        ("max_hits", C.c_uint32),
+        ("graph", C.c_uint32),
+        ("memory_budget", C.c_uint64),
+    ]
+
+
+class BatchHit(C.Structure):
+    _fields_ = [
+        ("search_id", C.c_uint64),
+        ("offset", C.c_uint64),
+        ("packed", C.c_uint8 * 32),
+        ("public_key", C.c_uint8 * 32),
+        ("filter", C.c_uint32),
+        ("pad", C.c_uint32),
+    ]
+
+
+class SearchStatus(C.Structure):
+    _fields_ = [
+        ("windows", C.c_uint64),
+        ("candidates", C.c_uint64),
+        ("hits", C.c_uint64),
+        ("lanes", C.c_uint32),
+        ("quota", C.c_uint32),
+        ("done", C.c_uint32),
+        ("filters", C.c_uint32),
+        ("table_bytes", C.c_uint64),
+    ]
+
+
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
@@ -83,6 +119,19 @@ def _load():
     sig("og_engine_advance", I, [P, P, SZ, C.POINTER(SZ), B, SZ])
     sig("og_engine_last_kernel_ms", C.c_float, [P])
     sig("og_engine_free", None, [P])
+    sig("og_batch_new", I, [I, C.POINTER(BatchConfig), C.POINTER(P), B, SZ])
+    sig("og_batch_admit", I, [P, U64, B, B, U32, B, SZ])
+    sig("og_batch_step", I, [P, P, SZ, C.POINTER(SZ), B, SZ])
+    sig("og_batch_room", SZ, [P])
+    sig("og_batch_status", I, [P, U64, C.POINTER(SearchStatus)])
+    sig("og_batch_results", I, [P, U64, P, SZ, C.POINTER(SZ)])
+    sig("og_batch_retire", I, [P, U64])
+    sig("og_batch_counts", None, [P, C.POINTER(SZ), C.POINTER(SZ)])
+    sig("og_batch_last_step_ms", C.c_float, [P])
+    sig("og_batch_last_step_candidates", U64, [P])
+    sig("og_batch_last_step_launches", U32, [P])
+    sig("og_batch_memory", None, [P, C.POINTER(U64), C.POINTER(U64)])
+    sig("og_batch_free", None, [P])
     sig("og_measure_int_peak", I, [I, C.POINTER(C.c_double), C.POINTER(C.c_double), B, SZ])
     sig("og_secret_scalar", None, [B, B])
     sig("og_expanded_secret_key", None, [B, B])

@@ -1,0 +1,735 @@
+// og_batch: many independent searches advancing together in one persistent
+// kernel, replayed as a CUDA graph per step. No counterpart in the reference;
+// the per-search arithmetic is the single engine's paired round.
+//
+// Candidate windows. Window w of a search is the round centred on
+// scalar offset 8 (w (2 half + 1) + half + 1): its 2 half + 1 candidates are
+// offsets 8 (w (2 half + 1) + 1 + i), i in [0, 2 half]. A search holding L
+// lanes for a step of R rounds processes windows [W, W + R L) — lane l takes
+// W + r L + l in round r — and ends the step with lane l centred on window
+// W + R L + l. So after every step lane l sits on window W_done + l whatever
+// L was: a search that grows only initialises its new lanes, one that
+// shrinks drops its highest lanes, and the windows it has processed are
+// always exactly [0, W_done).
+//
+// Results. A search is done when it holds `quota` verified hits; because its
+// windows are processed in increasing order, these are its first `quota`
+// hits in offset order, a pure function of the search alone.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cstddef>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/onion_gen_b200.h"
+#include "host/common.h"
+#include "host/filters.h"
+#include "host/keys.h"
+#include "search_common.cuh"
+
+#ifndef OG_LB_THREADS
+#define OG_LB_THREADS 128
+#endif
+#ifndef OG_LB_MIN_BLOCKS
+#define OG_LB_MIN_BLOCKS 6
+#endif
+
+namespace og {
+
+const std::vector<uint4>& pair_table(uint32_t half);           // engine.cu
+std::vector<uint4> pow2_table(const Pt& stride, uint32_t nbits);  // engine.cu
+
+namespace {
+
+constexpr uint32_t BLOCK = 128;
+constexpr uint32_t NONE = 0xffffffffu;
+constexpr int MAX_BUCKETS = 12;
+constexpr uint32_t POW2_BITS = 24;  // lanes of one search stay below 2^24
+// A filter set whose bitmap lets more than this fraction of candidates
+// through is refused: the survivor buffer is sized from it.
+constexpr double MAX_OCCUPANCY = 0.02;
+
+struct BatchDesc {
+    FeWords wx, wy, wt;      // the search's stride for this step: L (2 half + 1) 8 G, affine
+    FeWords bx, by, bz, bt;  // centre of window W_done (where new lanes start), extended
+    const uint32_t* bitmap;
+    const uint64_t* keys;
+    const uint32_t* owners;
+    uint32_t bits;
+    uint32_t nbuckets;
+    uint32_t bucket_bits[MAX_BUCKETS];
+    uint32_t bucket_off[MAX_BUCKETS];
+    uint32_t bucket_len[MAX_BUCKETS];
+};
+
+struct SlotBlock {
+    uint32_t sidx;   // descriptor index, NONE when the block is idle
+    uint32_t lane0;  // lane index (within its search) of the block's first slot
+};
+
+struct Counters {
+    uint32_t work;        // next work item of the persistent kernel
+    uint32_t init_count;  // slot blocks in the init list
+    uint32_t surv;        // bitmap survivors written
+    uint32_t hits;        // exact hits written
+};
+
+struct BatchArgs {
+    const BatchDesc* descs;
+    const SlotBlock* blocks;
+    const uint32_t* init_list;
+    Counters* counters;
+    uint32_t nblocks;
+    uint4* lanes;  // ({x,y} * 2 + q) * slots + slot
+    uint4* scratch;
+    size_t slots;
+    const uint4* table;
+    const uint4* pow2;
+    uint32_t half;
+    uint32_t rounds;
+    HitRec* surv;
+    uint32_t surv_cap;
+    HitRec* hits;
+    uint32_t hit_cap;
+};
+
+__global__ void __launch_bounds__(BLOCK) batch_init_kernel(const BatchArgs a) {
+    if (blockIdx.x >= a.counters->init_count) return;
+    const uint32_t b = a.init_list[blockIdx.x];
+    const SlotBlock sb = a.blocks[b];
+    const BatchDesc& d = a.descs[sb.sidx];
+    const uint32_t lane = sb.lane0 + threadIdx.x;
+    const size_t slot = (size_t)b * BLOCK + threadIdx.x;
+    fe X = words_fe(d.bx), Y = words_fe(d.by), Z = words_fe(d.bz), T = words_fe(d.bt);
+    for (uint32_t k = 0; k < POW2_BITS; k++) {
+        if ((lane >> k) & 1u) {
+            const uint4* p = a.pow2 + (size_t)k * 6;
+            add_cached(X, Y, Z, T, load_fe(p + 0, 1), load_fe(p + 2, 1), load_fe(p + 4, 1));
+        }
+    }
+    const fe zi = fe_invert(Z);
+    store_fe(a.lanes + 0 * a.slots + slot, a.slots, fe_mulv(X, zi));
+    store_fe(a.lanes + 2 * a.slots + slot, a.slots, fe_mulv(Y, zi));
+}
+
+// Persistent: one CTA per resident slot, each pulling slot blocks until the
+// pool is exhausted. Every block of lanes belongs to one search, whose
+// descriptor gives its stride and bitmap.
+__global__ void __launch_bounds__(OG_LB_THREADS, OG_LB_MIN_BLOCKS) batch_search_kernel(const BatchArgs a) {
+    extern __shared__ uint4 qtab[];
+    __shared__ uint32_t item_s;
+    for (uint32_t i = threadIdx.x; i < a.half * 6; i += blockDim.x) qtab[i] = a.table[i];
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) item_s = atomicAdd(&a.counters->work, 1u);
+        __syncthreads();
+        const uint32_t item = item_s;
+        if (item >= a.nblocks) break;
+        const SlotBlock sb = a.blocks[item];
+        if (sb.sidx == NONE) continue;
+        const BatchDesc& d = a.descs[sb.sidx];
+        const uint32_t slot = item * BLOCK + threadIdx.x;
+        const Sink sink{d.bitmap, d.bits, a.surv, &a.counters->surv, a.surv_cap, sb.sidx};
+        fe x = load_fe(a.lanes + 0 * a.slots + slot, a.slots);
+        fe y = load_fe(a.lanes + 2 * a.slots + slot, a.slots);
+        paired_rounds(x, y, words_fe(d.wx), words_fe(d.wy), words_fe(d.wt), qtab, a.half, a.rounds,
+                      a.scratch + slot, a.slots, [&](const fe& v, uint32_t step) { test_emit(sink, v, slot, step); });
+        store_fe(a.lanes + 0 * a.slots + slot, a.slots, x);
+        store_fe(a.lanes + 2 * a.slots + slot, a.slots, y);
+    }
+}
+
+// Exact match of the bitmap survivors: per distinct filter length, a binary
+// search of the sorted masked key heads (FilterSet::match_key on the device).
+__global__ void __launch_bounds__(256) batch_exact_kernel(const BatchArgs a) {
+    const uint32_t n = min(a.counters->surv, a.surv_cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const HitRec r = a.surv[i];
+        const BatchDesc& d = a.descs[r.search];
+        const uint64_t head =
+            ((uint64_t)__byte_perm(r.y[0], 0, 0x0123) << 32) | (uint64_t)__byte_perm(r.y[1], 0, 0x0123);
+        for (uint32_t b = 0; b < d.nbuckets; b++) {
+            const uint64_t probe = head & (~0ULL << (64 - d.bucket_bits[b]));
+            const uint64_t* k = d.keys + d.bucket_off[b];
+            uint32_t lo = 0, hi = d.bucket_len[b];
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (k[mid] < probe) lo = mid + 1;
+                else hi = mid;
+            }
+            if (lo < d.bucket_len[b] && k[lo] == probe) {
+                const uint32_t idx = atomicAdd(&a.counters->hits, 1u);
+                if (idx < a.hit_cap) {
+                    HitRec h = r;
+                    h.pad = d.owners[d.bucket_off[b] + lo];
+                    a.hits[idx] = h;
+                }
+                break;
+            }
+        }
+    }
+}
+
+struct Search {
+    uint64_t id = 0;
+    uint8_t seed[32];
+    uint8_t scalar[32];
+    Pt start;
+    FilterSet fs;
+    bool long_filters = false;
+    uint32_t quota = 0;
+    uint32_t sidx = NONE;
+    DevBuf<uint32_t> bitmap;
+    DevBuf<uint64_t> keys;
+    DevBuf<uint32_t> owners;
+    std::vector<FilterSet::DeviceBucket> buckets;
+    uint64_t table_bytes = 0;
+    uint64_t windows = 0;           // W_done
+    std::vector<uint32_t> blocks;   // slot blocks held, in lane order
+    uint32_t lanes_last = 0;        // lanes held in the last step
+    uint32_t lanes_stride = 0;      // lane count the descriptor's stride is for
+    std::vector<og_batch_hit> hits; // verified, in offset order
+    bool done = false;
+    uint64_t admit_order = 0;
+};
+
+}  // namespace
+}  // namespace og
+
+using namespace og;
+
+struct og_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    og_batch_config cfg{};
+    uint32_t slots = 0, nblocks = 0, grid = 0;
+    size_t smem = 0;
+    DevBuf<uint4> lanes, scratch, table, pow2;
+    DevBuf<BatchDesc> descs;
+    DevBuf<SlotBlock> blocks;
+    DevBuf<uint32_t> init_list;
+    DevBuf<Counters> counters;
+    DevBuf<HitRec> surv, hits;
+    HostBuf<BatchDesc> h_descs;
+    HostBuf<SlotBlock> h_blocks;
+    HostBuf<uint32_t> h_init;
+    HostBuf<Counters> h_counters;
+    HostBuf<HitRec> h_hits;
+    std::map<uint64_t, std::unique_ptr<Search>> searches;
+    std::vector<uint32_t> free_sidx;
+    std::vector<uint32_t> free_blocks;
+    std::map<uint32_t, std::array<FeWords, 3>> strides;  // per lane count
+    uint64_t admitted = 0;
+    uint64_t mem_used = 0, mem_budget = 0;
+    uint64_t mismatches = 0;
+    bool active_changed = true;
+    float last_ms = 0;
+    uint64_t last_candidates = 0;
+    uint32_t last_launches = 0;
+    uint32_t dirty_lo = NONE, dirty_hi = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    BatchArgs args{};
+
+    ~og_batch() {
+        if (stream) cudaStreamSynchronize(stream);
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        searches.clear();
+        if (stream) cudaStreamDestroy(stream);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+    }
+
+    void mark(uint32_t sidx) {
+        dirty_lo = std::min(dirty_lo, sidx);
+        dirty_hi = std::max(dirty_hi, sidx + 1);
+    }
+};
+
+namespace {
+
+#define CU(call)                                                                                 \
+    do {                                                                                         \
+        cudaError_t _e = (call);                                                                 \
+        if (_e != cudaSuccess)                                                                   \
+            return fail(err, errlen, _e == cudaErrorMemoryAllocation ? OG_E_NOMEM : OG_E_DEVICE, \
+                        "%s: %s", #call, cuda_text(_e).c_str());                                 \
+    } while (0)
+
+const std::array<FeWords, 3>& stride_for(og_batch* b, uint32_t lanes) {
+    auto it = b->strides.find(lanes);
+    if (it != b->strides.end()) return it->second;
+    F51 x, y;
+    pt_affine(base_mult_u64(8ULL * (2ULL * b->cfg.half + 1) * lanes), x, y);
+    std::array<FeWords, 3> w{to_words(x), to_words(y), to_words(f_mul(x, y))};
+    return b->strides.emplace(lanes, w).first->second;
+}
+
+// Window W's centre for search s: s * B + 8 (W (2 half + 1) + half + 1) B.
+Pt window_centre(const og_batch* b, const Search& s, uint64_t w) {
+    const uint64_t k = 8ULL * (w * (2ULL * b->cfg.half + 1) + b->cfg.half + 1);
+    return pt_add(s.start, base_mult_u64(k));
+}
+
+void release_blocks(og_batch* b, Search& s) {
+    for (uint32_t blk : s.blocks) b->free_blocks.push_back(blk);
+    s.blocks.clear();
+}
+
+// Shares the slot pool equally among unfinished searches (the earliest
+// admitted first when there are more searches than blocks). Searches above
+// their share drop their highest blocks; those below take free blocks, whose
+// lanes are queued for initialisation.
+void rebalance(og_batch* b, std::vector<uint32_t>& init) {
+    std::vector<Search*> running;
+    for (auto& kv : b->searches)
+        if (!kv.second->done) running.push_back(kv.second.get());
+    std::sort(running.begin(), running.end(), [](Search* x, Search* y) { return x->admit_order < y->admit_order; });
+    const size_t n_sched = std::min<size_t>(running.size(), b->nblocks);
+    std::vector<uint32_t> target(running.size(), 0);
+    for (size_t i = 0; i < n_sched; i++)
+        target[i] = (uint32_t)(b->nblocks / n_sched + (i < b->nblocks % n_sched ? 1 : 0));
+    for (size_t i = 0; i < running.size(); i++) {
+        Search& s = *running[i];
+        while (s.blocks.size() > target[i]) {
+            b->free_blocks.push_back(s.blocks.back());
+            s.blocks.pop_back();
+        }
+    }
+    for (size_t i = 0; i < running.size(); i++) {
+        Search& s = *running[i];
+        const size_t had = s.blocks.size();
+        while (s.blocks.size() < target[i] && !b->free_blocks.empty()) {
+            s.blocks.push_back(b->free_blocks.back());
+            b->free_blocks.pop_back();
+        }
+        if (s.blocks.size() > had) {
+            // the new lanes start on windows W_done + lane
+            const Pt c = window_centre(b, s, s.windows);
+            BatchDesc& d = b->h_descs.p[s.sidx];
+            d.bx = to_words(c.X);
+            d.by = to_words(c.Y);
+            d.bz = to_words(c.Z);
+            d.bt = to_words(c.T);
+            b->mark(s.sidx);
+            for (size_t j = had; j < s.blocks.size(); j++) init.push_back(s.blocks[j]);
+        }
+    }
+    // the block table
+    for (uint32_t i = 0; i < b->nblocks; i++) b->h_blocks.p[i] = SlotBlock{NONE, 0};
+    for (Search* s : running)
+        for (size_t j = 0; j < s->blocks.size(); j++) b->h_blocks.p[s->blocks[j]] = SlotBlock{s->sidx, (uint32_t)(j * BLOCK)};
+}
+
+int enqueue_step(og_batch* b, char* err, size_t errlen) {
+    CU(cudaMemsetAsync(b->counters.p, 0, offsetof(Counters, init_count), b->stream));
+    CU(cudaMemsetAsync(&b->counters.p->surv, 0, 2 * sizeof(uint32_t), b->stream));
+    batch_init_kernel<<<b->nblocks, BLOCK, 0, b->stream>>>(b->args);
+    CU(cudaGetLastError());
+    batch_search_kernel<<<b->grid, BLOCK, b->smem, b->stream>>>(b->args);
+    CU(cudaGetLastError());
+    batch_exact_kernel<<<b->grid, 256, 0, b->stream>>>(b->args);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(b->h_counters.p, b->counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, b->stream));
+    return OG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int og_batch_new(int ordinal, const og_batch_config* cfgp, og_batch** out, char* err, size_t errlen) {
+    if (!out) return fail(err, errlen, OG_E_ARG, "null argument");
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+        return fail(err, errlen, OG_E_NODEVICE, "no CUDA device is available");
+    if (ordinal < 0 || ordinal >= count) return fail(err, errlen, OG_E_ARG, "device %d of %d", ordinal, count);
+    og_batch_config cfg{};
+    if (cfgp) cfg = *cfgp;
+    if (cfg.half == 0) cfg.half = 256;
+    if (cfg.half > 2048) return fail(err, errlen, OG_E_ARG, "half %u > 2048", cfg.half);
+    if (cfg.rounds == 0) cfg.rounds = 1;
+    if (cfg.max_searches == 0) cfg.max_searches = 4096;
+    if (cfg.graph > 2) return fail(err, errlen, OG_E_ARG, "graph mode %u", cfg.graph);
+    CU(cudaSetDevice(ordinal));
+    std::unique_ptr<og_batch> b(new (std::nothrow) og_batch());
+    if (!b) return fail(err, errlen, OG_E_NOMEM, "host memory");
+    b->device = ordinal;
+    b->smem = (size_t)cfg.half * 96;
+    if (b->smem > 48 * 1024)
+        CU(cudaFuncSetAttribute(batch_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+    int per_sm = 0, sms = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_search_kernel, BLOCK, b->smem));
+    CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ordinal));
+    b->grid = (uint32_t)std::max(1, per_sm) * (uint32_t)sms;
+    if (cfg.slots == 0) cfg.slots = 2 * b->grid * BLOCK;
+    cfg.slots = (cfg.slots + BLOCK - 1) / BLOCK * BLOCK;
+    b->slots = cfg.slots;
+    b->nblocks = cfg.slots / BLOCK;
+    const uint64_t per_step = (uint64_t)cfg.slots * (2ULL * cfg.half + 1) * cfg.rounds;
+    // survivors per step stay below MAX_OCCUPANCY of the candidates; four times that, at least 2^20
+    const uint64_t surv_cap = std::max<uint64_t>(1ULL << 20, (uint64_t)(4.0 * MAX_OCCUPANCY * (double)per_step));
+    if (surv_cap > 0xffffffffULL) return fail(err, errlen, OG_E_ARG, "a step of %llu candidates is too large", (unsigned long long)per_step);
+    if (cfg.max_hits == 0) cfg.max_hits = (uint32_t)surv_cap;
+    b->cfg = cfg;
+
+    CU(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    CU(cudaEventCreate(&b->ev0));
+    CU(cudaEventCreate(&b->ev1));
+    const size_t S = cfg.slots;
+    CU(b->lanes.alloc(S * 4));
+    CU(b->scratch.alloc(S * (2 * (size_t)cfg.half + 2) * 4));
+    const std::vector<uint4>& tab = pair_table(cfg.half);
+    CU(b->table.alloc(tab.size()));
+    CU(cudaMemcpyAsync(b->table.p, tab.data(), tab.size() * sizeof(uint4), cudaMemcpyHostToDevice, b->stream));
+    std::vector<uint4> pw = pow2_table(base_mult_u64(8ULL * (2ULL * cfg.half + 1)), POW2_BITS);
+    CU(b->pow2.alloc(pw.size()));
+    CU(cudaMemcpyAsync(b->pow2.p, pw.data(), pw.size() * sizeof(uint4), cudaMemcpyHostToDevice, b->stream));
+    CU(b->descs.alloc(cfg.max_searches));
+    CU(b->h_descs.alloc(cfg.max_searches));
+    std::memset(b->h_descs.p, 0, cfg.max_searches * sizeof(BatchDesc));
+    CU(b->blocks.alloc(b->nblocks));
+    CU(b->h_blocks.alloc(b->nblocks));
+    CU(b->init_list.alloc(b->nblocks));
+    CU(b->h_init.alloc(b->nblocks + 1));
+    CU(b->counters.alloc(1));
+    CU(b->h_counters.alloc(1));
+    CU(b->surv.alloc(surv_cap));
+    CU(b->hits.alloc(cfg.max_hits));
+    CU(b->h_hits.alloc(std::min<uint64_t>(cfg.max_hits, 1u << 16)));
+    for (uint32_t i = 0; i < b->nblocks; i++) {
+        b->h_blocks.p[i] = SlotBlock{NONE, 0};
+        b->free_blocks.push_back(b->nblocks - 1 - i);
+    }
+    for (uint32_t i = 0; i < cfg.max_searches; i++) b->free_sidx.push_back(cfg.max_searches - 1 - i);
+    CU(cudaMemcpyAsync(b->descs.p, b->h_descs.p, cfg.max_searches * sizeof(BatchDesc), cudaMemcpyHostToDevice, b->stream));
+    CU(cudaMemcpyAsync(b->blocks.p, b->h_blocks.p, b->nblocks * sizeof(SlotBlock), cudaMemcpyHostToDevice, b->stream));
+    CU(cudaStreamSynchronize(b->stream));
+    size_t free_b = 0, total_b = 0;
+    CU(cudaMemGetInfo(&free_b, &total_b));
+    b->mem_budget = cfg.memory_budget ? cfg.memory_budget : free_b / 2;
+
+    BatchArgs& a = b->args;
+    a.descs = b->descs.p;
+    a.blocks = b->blocks.p;
+    a.init_list = b->init_list.p;
+    a.counters = b->counters.p;
+    a.nblocks = b->nblocks;
+    a.lanes = b->lanes.p;
+    a.scratch = b->scratch.p;
+    a.slots = S;
+    a.table = b->table.p;
+    a.pow2 = b->pow2.p;
+    a.half = cfg.half;
+    a.rounds = cfg.rounds;
+    a.surv = b->surv.p;
+    a.surv_cap = (uint32_t)surv_cap;
+    a.hits = b->hits.p;
+    a.hit_cap = cfg.max_hits;
+
+    if (cfg.graph != 2) {
+        CU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_step(b.get(), err, errlen);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+        if (rc != OG_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        CU(e);
+        b->graph = g;
+        CU(cudaGraphInstantiate(&b->exec, g, 0));
+    }
+    *out = b.release();
+    return OG_OK;
+}
+
+int og_batch_admit(og_batch* b, uint64_t search_id, const uint8_t seed[32], const char* filters, uint32_t quota,
+                   char* err, size_t errlen) {
+    if (!b || !seed || !filters) return fail(err, errlen, OG_E_ARG, "null argument");
+    if (quota == 0) return fail(err, errlen, OG_E_ARG, "a quota of zero");
+    if (b->searches.count(search_id)) return fail(err, errlen, OG_E_STATE, "search %llu is already admitted", (unsigned long long)search_id);
+    if (b->free_sidx.empty()) return fail(err, errlen, OG_E_CAPACITY, "%u searches are admitted already", b->cfg.max_searches);
+    std::unique_ptr<Search> s(new (std::nothrow) Search());
+    if (!s) return fail(err, errlen, OG_E_NOMEM, "host memory");
+    s->id = search_id;
+    s->quota = quota;
+    std::memcpy(s->seed, seed, 32);
+    secret_scalar(seed, s->scalar);
+    s->start = base_mult(s->scalar);
+    // filters
+    std::vector<PrefixFilter> fs;
+    const char* p = filters;
+    size_t line = 0;
+    while (*p) {
+        const char* e = std::strchr(p, '\n');
+        std::string text = e ? std::string(p, (size_t)(e - p)) : std::string(p);
+        line++;
+        if (text.find_first_not_of(" \t\r") != std::string::npos) {
+            PrefixFilter f;
+            std::string why;
+            if (!parse_prefix(text, f, why)) return fail(err, errlen, OG_E_FILTER, "line %zu: %s", line, why.c_str());
+            fs.push_back(f);
+        }
+        if (!e) break;
+        p = e + 1;
+    }
+    std::string why;
+    if (!s->fs.build(std::move(fs), 0, why)) return fail(err, errlen, OG_E_FILTER, "%s", why.c_str());
+    if (s->fs.occupancy() > MAX_OCCUPANCY)
+        return fail(err, errlen, OG_E_FILTER, "the filters leave %.1f%% of the index set (at most %.0f%% in a batch)",
+                    100 * s->fs.occupancy(), 100 * MAX_OCCUPANCY);
+    for (size_t i = 0; i < s->fs.size(); i++)
+        if (s->fs.filter(i).text.size() > FilterSet::DEVICE_SYMBOLS) s->long_filters = true;
+    std::vector<uint64_t> keys;
+    std::vector<uint32_t> owners;
+    s->fs.device_tables(s->buckets, keys, owners);
+    if (s->buckets.size() > MAX_BUCKETS) return fail(err, errlen, OG_E_FILTER, "more than %d filter lengths", MAX_BUCKETS);
+    const size_t words32 = s->fs.words().size() * 2;
+    s->table_bytes = words32 * 4 + keys.size() * 12;
+    if (b->mem_used + s->table_bytes > b->mem_budget)
+        return fail(err, errlen, OG_E_NOMEM, "its tables (%llu bytes) do not fit the remaining budget (%llu of %llu used)",
+                    (unsigned long long)s->table_bytes, (unsigned long long)b->mem_used, (unsigned long long)b->mem_budget);
+    CU(cudaSetDevice(b->device));
+    CU(s->bitmap.alloc(words32));
+    CU(s->keys.alloc(keys.size()));
+    CU(s->owners.alloc(owners.size()));
+    CU(cudaMemcpyAsync(s->bitmap.p, s->fs.words().data(), words32 * 4, cudaMemcpyHostToDevice, b->stream));
+    CU(cudaMemcpyAsync(s->keys.p, keys.data(), keys.size() * 8, cudaMemcpyHostToDevice, b->stream));
+    CU(cudaMemcpyAsync(s->owners.p, owners.data(), owners.size() * 4, cudaMemcpyHostToDevice, b->stream));
+    CU(cudaStreamSynchronize(b->stream));
+    s->sidx = b->free_sidx.back();
+    b->free_sidx.pop_back();
+    BatchDesc& d = b->h_descs.p[s->sidx];
+    std::memset(&d, 0, sizeof d);
+    d.bitmap = s->bitmap.p;
+    d.keys = s->keys.p;
+    d.owners = s->owners.p;
+    d.bits = s->fs.bits();
+    d.nbuckets = (uint32_t)s->buckets.size();
+    for (size_t i = 0; i < s->buckets.size(); i++) {
+        d.bucket_bits[i] = s->buckets[i].bits;
+        d.bucket_off[i] = s->buckets[i].offset;
+        d.bucket_len[i] = s->buckets[i].count;
+    }
+    b->mark(s->sidx);
+    s->admit_order = b->admitted++;
+    b->mem_used += s->table_bytes;
+    b->searches[search_id] = std::move(s);
+    b->active_changed = true;
+    return OG_OK;
+}
+
+size_t og_batch_room(const og_batch* b) { return b ? b->cfg.max_hits : 0; }
+
+int og_batch_step(og_batch* b, og_batch_hit* out, size_t cap, size_t* n, char* err, size_t errlen) {
+    if (!b || !n) return fail(err, errlen, OG_E_ARG, "null argument");
+    *n = 0;
+    b->last_ms = 0;
+    b->last_candidates = 0;
+    b->last_launches = 0;
+    CU(cudaSetDevice(b->device));
+    std::vector<uint32_t> init;
+    if (b->active_changed) {
+        rebalance(b, init);
+        b->active_changed = false;
+    }
+    // strides for this step's lane counts
+    std::vector<Search*> sched;
+    for (auto& kv : b->searches) {
+        Search& s = *kv.second;
+        if (s.done || s.blocks.empty()) continue;
+        sched.push_back(&s);
+        const uint32_t lanes = (uint32_t)s.blocks.size() * BLOCK;
+        if (lanes != s.lanes_stride) {
+            const auto& w = stride_for(b, lanes);
+            BatchDesc& d = b->h_descs.p[s.sidx];
+            d.wx = w[0];
+            d.wy = w[1];
+            d.wt = w[2];
+            s.lanes_stride = lanes;
+            b->mark(s.sidx);
+        }
+    }
+    if (sched.empty()) return OG_OK;
+    if (b->dirty_lo < b->dirty_hi) {
+        CU(cudaMemcpyAsync(b->descs.p + b->dirty_lo, b->h_descs.p + b->dirty_lo,
+                           (b->dirty_hi - b->dirty_lo) * sizeof(BatchDesc), cudaMemcpyHostToDevice, b->stream));
+        b->dirty_lo = NONE;
+        b->dirty_hi = 0;
+    }
+    CU(cudaMemcpyAsync(b->blocks.p, b->h_blocks.p, b->nblocks * sizeof(SlotBlock), cudaMemcpyHostToDevice, b->stream));
+    for (size_t i = 0; i < init.size(); i++) b->h_init.p[i] = init[i];
+    if (!init.empty())
+        CU(cudaMemcpyAsync(b->init_list.p, b->h_init.p, init.size() * 4, cudaMemcpyHostToDevice, b->stream));
+    b->h_init.p[b->nblocks] = (uint32_t)init.size();
+    CU(cudaMemcpyAsync(&b->counters.p->init_count, &b->h_init.p[b->nblocks], 4, cudaMemcpyHostToDevice, b->stream));
+    CU(cudaEventRecord(b->ev0, b->stream));
+    if (b->exec) {
+        CU(cudaGraphLaunch(b->exec, b->stream));
+    } else {
+        int rc = enqueue_step(b, err, errlen);
+        if (rc != OG_OK) return rc;
+    }
+    CU(cudaEventRecord(b->ev1, b->stream));
+    CU(cudaStreamSynchronize(b->stream));
+    cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1);
+    b->last_launches = 3;
+    const Counters c = *b->h_counters.p;
+    if (c.surv > b->args.surv_cap || c.hits > b->args.hit_cap)
+        return fail(err, errlen, OG_E_OVERFLOW, "a step produced %u survivors (room %u) and %u hits (room %u)", c.surv,
+                    b->args.surv_cap, c.hits, b->args.hit_cap);
+    // copy the exact hits back in chunks
+    std::vector<HitRec> recs(c.hits);
+    const size_t chunk = b->h_hits.n;
+    for (size_t off = 0; off < c.hits; off += chunk) {
+        const size_t m = std::min<size_t>(chunk, c.hits - off);
+        CU(cudaMemcpyAsync(b->h_hits.p, b->hits.p + off, m * sizeof(HitRec), cudaMemcpyDeviceToHost, b->stream));
+        CU(cudaStreamSynchronize(b->stream));
+        std::memcpy(recs.data() + off, b->h_hits.p, m * sizeof(HitRec));
+    }
+    // decode offsets per search
+    const uint64_t slots_per_window = 2ULL * b->cfg.half + 1;
+    std::vector<Search*> by_sidx(b->cfg.max_searches, nullptr);
+    for (Search* s : sched) by_sidx[s->sidx] = s;
+    std::map<Search*, std::vector<og_batch_hit>> found;
+    for (const HitRec& h : recs) {
+        const uint32_t blk = h.lane / BLOCK;
+        const SlotBlock sb = b->h_blocks.p[blk];
+        Search* s = sb.sidx < by_sidx.size() ? by_sidx[sb.sidx] : nullptr;
+        if (!s || sb.sidx != h.search) continue;
+        const uint64_t lane = sb.lane0 + h.lane % BLOCK;
+        const uint64_t L = (uint64_t)s->blocks.size() * BLOCK;
+        const uint64_t r = h.step / slots_per_window, i = h.step % slots_per_window;
+        const uint64_t w = s->windows + r * L + lane;
+        og_batch_hit o{};
+        o.search_id = s->id;
+        o.offset = 8 * (w * slots_per_window + 1 + i);
+        for (int k = 0; k < 8; k++)
+            for (int j = 0; j < 4; j++) o.packed[4 * k + j] = (uint8_t)(h.y[k] >> (8 * j));
+        o.filter = h.pad;
+        found[s].push_back(o);
+    }
+    // advance, verify in offset order up to the quota
+    size_t emitted = 0;
+    uint64_t candidates = 0;
+    for (Search* s : sched) {
+        const uint64_t L = (uint64_t)s->blocks.size() * BLOCK;
+        s->lanes_last = (uint32_t)L;
+        s->windows += (uint64_t)b->cfg.rounds * L;
+        candidates += (uint64_t)b->cfg.rounds * L * slots_per_window;
+        auto it = found.find(s);
+        if (it == found.end()) continue;
+        std::vector<og_batch_hit>& v = it->second;
+        std::sort(v.begin(), v.end(), [](const og_batch_hit& x, const og_batch_hit& y) { return x.offset < y.offset; });
+        for (og_batch_hit& h : v) {
+            if (s->hits.size() >= s->quota) break;
+            if (s->long_filters) {
+                const long f = s->fs.match_key(h.packed);
+                if (f < 0) continue;
+                h.filter = (uint32_t)f;
+            }
+            uint8_t pk[32];
+            if (check_hit_scalar(s->scalar, h.offset, h.packed, pk) != HitCheck::ok) {
+                b->mismatches++;
+                continue;
+            }
+            std::memcpy(h.public_key, pk, 32);
+            // filters longer than the key-only span are confirmed on the address
+            const PrefixFilter& f = s->fs.filter(h.filter);
+            if (f.needs_full_check() && address(pk).compare(0, f.text.size(), f.text) != 0) continue;
+            s->hits.push_back(h);
+            if (out && emitted < cap) out[emitted] = h;
+            emitted++;
+        }
+        if (s->hits.size() >= s->quota) {
+            s->done = true;
+            release_blocks(b, *s);
+            b->active_changed = true;
+        }
+    }
+    b->last_candidates = candidates;
+    *n = std::min(emitted, cap);
+    if (b->mismatches)
+        return fail(err, errlen, OG_E_VERIFY, "%llu device hits did not re-derive on the host",
+                    (unsigned long long)b->mismatches);
+    if (emitted > cap) return fail(err, errlen, OG_E_CAPACITY, "%zu hits and room for %zu", emitted, cap);
+    return OG_OK;
+}
+
+int og_batch_status(const og_batch* b, uint64_t search_id, og_search_status* st) {
+    if (!b || !st) return OG_E_ARG;
+    auto it = b->searches.find(search_id);
+    if (it == b->searches.end()) return OG_E_STATE;
+    const Search& s = *it->second;
+    st->windows = s.windows;
+    st->candidates = s.windows * (2ULL * b->cfg.half + 1);
+    st->hits = s.hits.size();
+    st->lanes = s.lanes_last;
+    st->quota = s.quota;
+    st->done = s.done ? 1 : 0;
+    st->filters = (uint32_t)s.fs.size();
+    st->table_bytes = s.table_bytes;
+    return OG_OK;
+}
+
+int og_batch_results(const og_batch* b, uint64_t search_id, og_batch_hit* out, size_t cap, size_t* n) {
+    if (!b || !n) return OG_E_ARG;
+    *n = 0;
+    auto it = b->searches.find(search_id);
+    if (it == b->searches.end()) return OG_E_STATE;
+    const Search& s = *it->second;
+    if (cap < s.hits.size()) return OG_E_CAPACITY;
+    for (size_t i = 0; i < s.hits.size(); i++) out[i] = s.hits[i];
+    *n = s.hits.size();
+    return OG_OK;
+}
+
+int og_batch_retire(og_batch* b, uint64_t search_id) {
+    if (!b) return OG_E_ARG;
+    auto it = b->searches.find(search_id);
+    if (it == b->searches.end()) return OG_E_STATE;
+    Search& s = *it->second;
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+    release_blocks(b, s);
+    b->free_sidx.push_back(s.sidx);
+    b->mem_used -= s.table_bytes;
+    if (!s.done) b->active_changed = true;
+    b->searches.erase(it);
+    return OG_OK;
+}
+
+void og_batch_counts(const og_batch* b, size_t* admitted, size_t* running) {
+    size_t a = 0, r = 0;
+    if (b)
+        for (const auto& kv : b->searches) {
+            a++;
+            if (!kv.second->done) r++;
+        }
+    if (admitted) *admitted = a;
+    if (running) *running = r;
+}
+
+float og_batch_last_step_ms(const og_batch* b) { return b ? b->last_ms : 0.f; }
+uint64_t og_batch_last_step_candidates(const og_batch* b) { return b ? b->last_candidates : 0; }
+uint32_t og_batch_last_step_launches(const og_batch* b) { return b ? b->last_launches : 0; }
+
+void og_batch_memory(const og_batch* b, uint64_t* used, uint64_t* budget) {
+    if (used) *used = b ? b->mem_used : 0;
+    if (budget) *budget = b ? b->mem_budget : 0;
+}
+
+void og_batch_free(og_batch* b) { delete b; }
+
+}  // extern "C"

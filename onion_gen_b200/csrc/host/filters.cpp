@@ -216,6 +216,31 @@ long FilterSet::match_key(const uint8_t packed[32]) const {
     return -1;
 }
 
+void FilterSet::device_tables(std::vector<DeviceBucket>& buckets, std::vector<uint64_t>& keys,
+                              std::vector<uint32_t>& owners) const {
+    buckets.clear();
+    keys.clear();
+    owners.clear();
+    std::vector<std::vector<std::pair<uint64_t, uint32_t>>> by_len(DEVICE_SYMBOLS + 1);
+    for (size_t i = 0; i < filters_.size(); i++) {
+        const size_t sym = std::min(filters_[i].text.size(), DEVICE_SYMBOLS);
+        const uint32_t hb = (uint32_t)(sym * 5);
+        uint8_t padded[32] = {0};
+        std::memcpy(padded, filters_[i].bytes, filters_[i].nbytes);
+        by_len[sym].push_back({head64(padded) & (~0ULL << (64 - hb)), (uint32_t)i});
+    }
+    for (size_t sym = 1; sym <= DEVICE_SYMBOLS; sym++) {
+        auto& v = by_len[sym];
+        if (v.empty()) continue;
+        std::sort(v.begin(), v.end());
+        buckets.push_back(DeviceBucket{(uint32_t)(sym * 5), (uint32_t)keys.size(), (uint32_t)v.size()});
+        for (auto& kv : v) {
+            keys.push_back(kv.first);
+            owners.push_back(kv.second);
+        }
+    }
+}
+
 double FilterSet::match_probability() const {
     double p = 0;
     for (const PrefixFilter& f : filters_) p += std::pow(32.0, -(double)std::min(f.text.size(), KEY_ONLY_SYMBOLS));

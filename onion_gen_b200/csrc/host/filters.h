@@ -49,6 +49,20 @@ public:
     // expected fraction of candidates that match some filter exactly
     double match_probability() const;
 
+    // The exact-match tables in the form the device searches: one bucket
+    // per distinct length (capped at DEVICE_SYMBOLS symbols), each a sorted
+    // run of masked 64-bit key heads with the owning filter's index.
+    // Filters longer than DEVICE_SYMBOLS are matched on their first
+    // DEVICE_SYMBOLS symbols there and confirmed by match_key() on the host.
+    static constexpr size_t DEVICE_SYMBOLS = 12;
+    struct DeviceBucket {
+        uint32_t bits;    // significant leading bits of the head
+        uint32_t offset;  // into keys / owners
+        uint32_t count;
+    };
+    void device_tables(std::vector<DeviceBucket>& buckets, std::vector<uint64_t>& keys,
+                       std::vector<uint32_t>& owners) const;
+
 private:
     struct Bucket {
         size_t symbols;

@@ -1,0 +1,55 @@
+"""The device search loop of onion-gen's run driver (src/run.rs:1030-1119).
+
+``device_search`` drives one ``gpu.Engine`` the way ``run::device_worker``
+does: advance, confirm every survivor exactly against the filter set, re-derive
+the key of every match from its offset on the host and compare it with the
+device's bytes, and stop once ``quota`` hits are in hand. It returns the
+first ``quota`` hits in offset order: every advance covers the next contiguous
+range of offsets, so once the quota is reached nothing below the last examined
+offset is missing.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+from . import filter as F
+from . import gpu, key
+
+
+@dataclass(frozen=True)
+class Found:
+    offset: int
+    packed: bytes
+    public_key: bytes
+    filter: int
+
+
+def device_search(device, seed: bytes, prefixes, quota: int, threads: int = 0, config=None, max_advances=None):
+    fs = F.FilterSet.parse_all(prefixes)
+    words, bits = fs.index_words()
+    start = key.start_point(seed)
+    eng = gpu.Engine(device, start, threads=threads, bitmap=words, bitmap_bits=bits, config=config)
+    found = []
+    advances = 0
+    examined = 0
+    try:
+        while len(found) < quota:
+            if max_advances is not None and advances >= max_advances:
+                break
+            offsets, packed = eng.advance_raw()
+            advances += 1
+            examined += eng.batch()
+            for off, p in zip(offsets, packed):
+                b = bytes(p)
+                f = fs.match_key(b)
+                if f is None:
+                    continue  # the bitmap said maybe, the exact check said no
+                pk, _ = key.check_hit(seed, int(off), b)
+                text = fs.texts()[f]
+                if len(text) > 49 and not key.address(pk).startswith(text):
+                    continue
+                found.append(Found(int(off), b, pk, f))
+    finally:
+        eng.close()
+    found.sort(key=lambda h: h.offset)
+    return found[:quota], examined, advances

@@ -1,0 +1,145 @@
+"""The batched engine on a B200 (-m gpu): results identical alone, in a mix,
+with and without graph replay, and to the single-search engine; every hit
+re-derived by the oracle; the first hits really are the first."""
+import numpy as np
+import pytest
+
+from onion_gen_b200 import _native as N
+from onion_gen_b200 import batch as B
+from onion_gen_b200 import run, workloads
+
+pytestmark = pytest.mark.gpu
+
+SEARCHES = [
+    (101, ["ab", "cd"], 5),
+    (102, ["xyz"], 3),
+    (103, [workloads.SplitMix64(77 + i).prefix(4, 4) for i in range(200)], 8),
+    (104, ["q7", "lmn", "uvwx"], 4),
+    (105, ["k2"], 16),
+    (106, [workloads.SplitMix64(9).prefix(5, 5)], 1),
+]
+SMALL = dict(half=64, slots=128 * 64)
+
+
+def key_of(h):
+    return (h.offset, h.packed)
+
+
+def run_batch(device, searches, **kw):
+    b = B.Batch(device, **{**SMALL, **kw})
+    for sid, prefixes, quota in searches:
+        b.admit(sid, workloads.seed(sid), prefixes, quota)
+    steps = 0
+    while b.running():
+        b.step()
+        steps += 1
+        assert steps < 5000
+    out = {sid: [key_of(h) for h in b.results(sid)] for sid, _, _ in searches}
+    for sid, _, quota in searches:
+        st = b.status(sid)
+        assert st.done == 1 and st.hits == quota
+    b.close()
+    return out, steps
+
+
+@pytest.fixture(scope="module")
+def mixed(device):
+    return run_batch(device, SEARCHES)
+
+
+def test_mixed_equals_alone(device, mixed):
+    out, steps = mixed
+    assert steps > 1
+    for s in SEARCHES:
+        alone, _ = run_batch(device, [s])
+        assert alone[s[0]] == out[s[0]], s[0]
+
+
+def test_graph_and_plain_launches_agree(device, mixed):
+    out, _ = mixed
+    plain, _ = run_batch(device, SEARCHES, graph=False)
+    assert plain == out
+
+
+def test_other_shapes_agree(device, mixed):
+    """Lane count, rounds per step and pool size change how much is examined,
+    never which hits come first."""
+    out, _ = mixed
+    other, _ = run_batch(device, SEARCHES, slots=128 * 23, rounds=3)
+    assert other == out
+
+
+def test_single_engine_agrees(device, mixed):
+    out, _ = mixed
+    for sid, prefixes, quota in SEARCHES:
+        cfg = N.EngineConfig(0, 64, 1024, 2, 128, 0, 0)
+        found, _, _ = run.device_search(device, workloads.seed(sid), prefixes, quota, config=cfg)
+        assert [(h.offset, h.packed) for h in found] == out[sid], sid
+
+
+def test_every_hit_rederives_in_the_oracle(device, oracle, mixed):
+    out, _ = mixed
+    for sid, prefixes, quota in SEARCHES:
+        seed = workloads.seed(sid)
+        fs = oracle.FilterSet(prefixes)
+        for off, packed in out[sid]:
+            sec = oracle.expanded_secret_at_offset(seed, off)
+            pk = oracle.pack(oracle.scalar_base_mult(sec[:32]))
+            assert pk[:31] == packed[:31] and pk[31] & 0x7F == packed[31]
+            assert fs.match(packed) >= 0
+
+
+def test_first_hits_are_the_first(device, oracle, mixed):
+    """An oracle scan of the first candidates finds exactly the same first
+    hits (offsets start at 8 and every multiple of 8 is examined)."""
+    out, _ = mixed
+    for sid, prefixes, quota in SEARCHES[:2] + SEARCHES[3:5]:
+        seed = workloads.seed(sid)
+        start = oracle.scalar_base_mult(oracle.secret_scalar(seed))
+        fs = oracle.FilterSet(prefixes)
+        want = []
+        first = 1
+        while len(want) < quota:
+            n = 1 << 18
+            keys = np.frombuffer(oracle.chain_keys_mt(start, first, n), dtype=np.uint8).reshape(-1, 32)
+            for i in range(n):
+                k = bytes(keys[i])
+                if fs.match(k) >= 0:
+                    want.append((8 * (first + i), k))
+                    if len(want) == quota:
+                        break
+            first += n
+        assert want == out[sid], sid
+
+
+def test_admission_by_memory(device):
+    b = B.Batch(device, memory_budget=40_000, **SMALL)
+    b.admit(1, workloads.seed(1), ["ab"], 1)  # a 16-bit index: 8 KiB
+    with pytest.raises(N.OgError) as e:
+        b.admit(2, workloads.seed(2), [workloads.SplitMix64(3).prefix(6, 6) for _ in range(3000)], 1)
+    assert e.value.status == "OG_E_NOMEM"
+    assert b.counts() == (1, 1)
+    used, budget = b.memory()
+    assert 0 < used <= budget == 40_000
+    b.retire(1)
+    assert b.memory()[0] == 0
+
+
+def test_retire_mid_search_and_errors(device):
+    b = B.Batch(device, **SMALL)
+    b.admit(7, workloads.seed(7), ["abcdefg"], 1)
+    b.admit(8, workloads.seed(8), ["ab"], 2)
+    b.step()
+    assert b.status(7).done == 0
+    b.retire(7)
+    with pytest.raises(N.OgError):
+        b.status(7)
+    with pytest.raises(N.OgError) as e:
+        b.admit(8, workloads.seed(8), ["ab"], 2)
+    assert e.value.status == "OG_E_STATE"
+    with pytest.raises(N.OgError) as e:
+        b.admit(9, workloads.seed(9), ["a0"], 2)
+    assert e.value.status == "OG_E_FILTER"
+    while b.running():
+        b.step()
+    assert len(b.results(8)) == 2

@@ -116,7 +116,8 @@ def test_admission_by_memory(device):
     b = B.Batch(device, memory_budget=40_000, **SMALL)
     b.admit(1, workloads.seed(1), ["ab"], 1)  # a 16-bit index: 8 KiB
     with pytest.raises(N.OgError) as e:
-        b.admit(2, workloads.seed(2), [workloads.SplitMix64(3).prefix(6, 6) for _ in range(3000)], 1)
+        r = workloads.SplitMix64(3)
+        b.admit(2, workloads.seed(2), [r.prefix(6, 6) for _ in range(3000)], 1)
     assert e.value.status == "OG_E_NOMEM"
     assert b.counts() == (1, 1)
     used, budget = b.memory()

@@ -189,6 +189,50 @@ uint32_t og_batch_last_step_launches(const og_batch* b);
 void og_batch_memory(const og_batch* b, uint64_t* used, uint64_t* budget);
 void og_batch_free(og_batch* b);
 
+/* ---- a search that allocates nothing ------------------------------------
+ *
+ * No counterpart in the reference. For callers that cannot allocate device
+ * memory — code inside another framework's memory pool, callers that must not
+ * synchronise the device (cudaMalloc and cudaFree can), processes that
+ * reserve all device memory up front — og_search_noalloc runs one paired
+ * search over a fixed range without calling cudaMalloc, cudaFree or any
+ * allocating library routine. The caller passes the inputs and outputs in
+ * device memory it owns; lane state, the Montgomery scratch and the tables
+ * live in one file-scope device array of OG_NOALLOC_SCRATCH_BYTES, which
+ * every GPU that loads this library holds until the process exits.
+ *
+ * It examines the first lanes * rounds * (2 half + 1) candidates of `start`
+ * (offsets 8 .. 8 N), exactly as og_engine_advance does on a fresh engine
+ * of the same shape, and writes each bitmap survivor (every candidate when
+ * `d_bitmap` is NULL) to `d_hits` (room `cap`) and their number to
+ * `*d_count` (zeroed by the call; a count above `cap` means records were
+ * dropped). A record's offset is 8 (w (2 half + 1) + 1 + i) with
+ * w = (step / (2 half + 1)) * lanes + lane and i = step % (2 half + 1).
+ *
+ * Limits: lanes a multiple of 128, half <= 512, and
+ * lanes * (2 half + 3) * 64 + (half + 24) * 96 <= OG_NOALLOC_SCRATCH_BYTES;
+ * beyond that the call fails with OG_E_CAPACITY before touching the device.
+ * Work is enqueued on `stream` (a cudaStream_t; NULL for the legacy default
+ * stream) and the call returns without waiting for it.
+ *
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Every call shares the one array: calls whose work overlaps on the GPU
+ * (different streams or host threads without ordering) race. */
+#define OG_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
+
+typedef struct og_hit_record {
+    uint32_t lane;
+    uint32_t step;
+    uint32_t search;
+    uint32_t reserved;
+    uint32_t y[8]; /* the packed key's little-endian words, sign bit clear */
+} og_hit_record;
+
+int og_search_noalloc(int ordinal, const uint8_t start[128], uint32_t lanes, uint32_t half, uint32_t rounds,
+                      const uint32_t* d_bitmap, uint32_t bits, og_hit_record* d_hits, uint32_t cap, uint32_t* d_count,
+                      void* stream, char* err, size_t errlen);
+
 /* ---- measurement --------------------------------------------------------- */
 
 /* The integer-multiply roofline of device `ordinal`, measured: the issue

@@ -132,6 +132,7 @@ def _load():
     sig("og_batch_last_step_launches", U32, [P])
     sig("og_batch_memory", None, [P, C.POINTER(U64), C.POINTER(U64)])
     sig("og_batch_free", None, [P])
+    sig("og_search_noalloc", I, [I, B, U32, U32, U32, P, U32, P, U32, P, P, B, SZ])
     sig("og_measure_int_peak", I, [I, C.POINTER(C.c_double), C.POINTER(C.c_double), B, SZ])
     sig("og_secret_scalar", None, [B, B])
     sig("og_expanded_secret_key", None, [B, B])

@@ -189,6 +189,60 @@ uint32_t og_batch_last_step_launches(const og_batch* b);
 void og_batch_memory(const og_batch* b, uint64_t* used, uint64_t* budget);
 void og_batch_free(og_batch* b);
 
+/* ---- serving: a request loop over the batched engine -------------------
+ *
+ * No counterpart in the reference. A worker thread owns one og_batch and
+ * runs steps continuously. Requests submitted from any thread wait in a FIFO
+ * queue and are admitted as lanes and device memory allow (a request the
+ * memory budget cannot take yet stays queued; one that can never parse
+ * completes with an error status). Each step advances every admitted request
+ * together; a request completes, and is retired, at the end of the step in
+ * which its quota of verified hits is reached. Its result is the same as if
+ * it had run alone (the batched engine's guarantee). Times are
+ * CLOCK_MONOTONIC nanoseconds. */
+
+typedef struct og_serve og_serve;
+
+typedef struct og_serve_config {
+    og_batch_config batch;  /* the engine the loop drives */
+    uint32_t max_running;   /* requests admitted at once (0: the batch's max_searches) */
+    uint32_t reserved;
+} og_serve_config;
+
+typedef struct og_serve_done {
+    uint64_t request_id;
+    uint64_t arrival_ns;   /* when og_serve_submit accepted it */
+    uint64_t admit_ns;     /* when it got a place on the device */
+    uint64_t done_ns;      /* end of the step that completed it */
+    uint64_t candidates;   /* candidates it examined */
+    uint32_t hits;         /* verified hits returned (its quota unless status != 0) */
+    uint32_t status;       /* og_status: OG_OK, or why it could not run */
+} og_serve_done;
+
+typedef struct og_serve_stats {
+    uint64_t steps;
+    uint64_t candidates;   /* all requests, all steps */
+    double device_ms;      /* sum of step device times */
+    uint64_t queued;       /* waiting for admission */
+    uint64_t running;      /* admitted, unfinished */
+    uint64_t completed;
+} og_serve_stats;
+
+int og_serve_new(int ordinal, const og_serve_config* cfg, og_serve** out, char* err, size_t errlen);
+/* Queues a request (thread-safe); the arrival time is taken here. */
+int og_serve_submit(og_serve* s, uint64_t request_id, const uint8_t seed[32], const char* filters, uint32_t quota,
+                    char* err, size_t errlen);
+/* Requests completed since the last poll, in completion order. */
+int og_serve_poll(og_serve* s, og_serve_done* out, size_t cap, size_t* n);
+/* The hits of a completed request (its first `quota` in offset order); they
+ * are kept until fetched once. */
+int og_serve_results(og_serve* s, uint64_t request_id, og_batch_hit* out, size_t cap, size_t* n);
+void og_serve_stats_get(og_serve* s, og_serve_stats* st);
+/* Nanoseconds on the clock the loop stamps with. */
+uint64_t og_serve_now_ns(void);
+/* Stops the loop (after its current step) and frees everything. */
+void og_serve_free(og_serve* s);
+
 /* ---- a search that allocates nothing ------------------------------------
  *
  * No counterpart in the reference. For callers that cannot allocate device

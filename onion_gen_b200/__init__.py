@@ -6,6 +6,6 @@ the hit path through the same library. Importing this package loads
 ``libonion_gen_b200.so`` and fails loudly if it is missing.
 """
 from . import _native  # noqa: F401  (loads the library or raises)
-from . import batch, filter, gpu, key  # noqa: F401
+from . import batch, filter, gpu, key, serve  # noqa: F401
 
-__all__ = ["gpu", "batch", "filter", "key"]
+__all__ = ["gpu", "batch", "serve", "filter", "key"]

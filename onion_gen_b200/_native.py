@@ -90,6 +90,33 @@ class SearchStatus(C.Structure):
     ]
 
 
+class ServeConfig(C.Structure):
+    _fields_ = [("batch", BatchConfig), ("max_running", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class ServeDone(C.Structure):
+    _fields_ = [
+        ("request_id", C.c_uint64),
+        ("arrival_ns", C.c_uint64),
+        ("admit_ns", C.c_uint64),
+        ("done_ns", C.c_uint64),
+        ("candidates", C.c_uint64),
+        ("hits", C.c_uint32),
+        ("status", C.c_uint32),
+    ]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [
+        ("steps", C.c_uint64),
+        ("candidates", C.c_uint64),
+        ("device_ms", C.c_double),
+        ("queued", C.c_uint64),
+        ("running", C.c_uint64),
+        ("completed", C.c_uint64),
+    ]
+
+
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
@@ -132,6 +159,13 @@ def _load():
     sig("og_batch_last_step_launches", U32, [P])
     sig("og_batch_memory", None, [P, C.POINTER(U64), C.POINTER(U64)])
     sig("og_batch_free", None, [P])
+    sig("og_serve_new", I, [I, C.POINTER(ServeConfig), C.POINTER(P), B, SZ])
+    sig("og_serve_submit", I, [P, U64, B, B, U32, B, SZ])
+    sig("og_serve_poll", I, [P, P, SZ, C.POINTER(SZ)])
+    sig("og_serve_results", I, [P, U64, P, SZ, C.POINTER(SZ)])
+    sig("og_serve_stats_get", None, [P, C.POINTER(ServeStats)])
+    sig("og_serve_now_ns", U64, [])
+    sig("og_serve_free", None, [P])
     sig("og_search_noalloc", I, [I, B, U32, U32, U32, P, U32, P, U32, P, P, B, SZ])
     sig("og_measure_int_peak", I, [I, C.POINTER(C.c_double), C.POINTER(C.c_double), B, SZ])
     sig("og_secret_scalar", None, [B, B])

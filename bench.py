@@ -19,6 +19,15 @@ One JSON line on rank 0:
   cpu_baseline the oracle's restatement of the reference's paired CPU engine
               (src/pairs.rs, batch 8192 as src/run.rs uses) on every host core
 
+  batched     config 4 (64 searches, 1..5000 prefixes of 4..7 symbols, quota
+              1..16): the single-search engine one search at a time (the
+              run driver's loop) against the batched engine, same results;
+              the default run takes the searches whose expected work is at
+              most --batched-cap candidates, --suite batched all of them
+  serving     config 5 (Poisson arrivals at 50/s, 1..200 prefixes, quota
+              1..16) through the serving loop: p50/p99 time-to-find over the
+              requests completed within a wall-clock cap
+
 --impl reference times that CPU engine alone (the reference's GPU engine is
 Rust compiled to PTX by a nightly toolchain that is not available here).
 Multi-GPU: one process per GPU; each rank searches its own disjoint offset
@@ -54,6 +63,13 @@ def parse():
     p.add_argument("--case", default="full", choices=["full", "small"],
                    help="small: the profiling case, three one-round advances of the plain engine")
     p.add_argument("--half", type=int, default=HALF)
+    p.add_argument("--suite", default="default", choices=["default", "batched", "serving", "plain"],
+                   help="default: the plain line plus bounded batched and serving legs; "
+                   "batched / serving: that leg at full size; plain: the plain line only")
+    p.add_argument("--batched-cap", type=float, default=2e10,
+                   help="largest expected work (candidates) of a config-4 search in the default run")
+    p.add_argument("--serving-requests", type=int, default=400)
+    p.add_argument("--serving-cap", type=float, default=20.0, help="serving wall-clock cap, seconds")
     return p.parse_args()
 
 
@@ -188,6 +204,105 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def batched_leg(dev, half, cap):
+    """Config 4: plain (one engine per search) against batched, same searches."""
+    from onion_gen_b200 import _native as N
+    from onion_gen_b200 import batch as B
+    from onion_gen_b200 import run, workloads
+
+    all_searches = workloads.config4_searches()
+    searches = [s for s in all_searches if s.expected_candidates() <= cap]
+    cfg = N.EngineConfig(N.SCHEME_PAIRED, half, 0, 0, 128, 0, 0)
+    t0 = time.perf_counter()
+    plain, plain_examined, plain_launches = {}, 0, 0
+    for s in searches:
+        found, examined, advances = run.device_search(dev, s.seed, s.prefixes, s.quota, config=cfg)
+        plain[s.index] = [(h.offset, h.packed) for h in found]
+        plain_examined += examined
+        plain_launches += 2 * advances + 1
+    plain_wall = time.perf_counter() - t0
+
+    t0 = time.perf_counter()
+    b = B.Batch(dev, half=half)
+    for s in searches:
+        b.admit(s.index, s.seed, s.prefixes, s.quota)
+    steps = launches = 0
+    dev_ms = 0.0
+    examined = 0
+    while b.running():
+        b.step()
+        steps += 1
+        launches += b.last_step_launches()
+        dev_ms += b.last_step_ms()
+        examined += b.last_step_candidates()
+    batched = {s.index: [(h.offset, h.packed) for h in b.results(s.index)] for s in searches}
+    b.close()
+    batched_wall = time.perf_counter() - t0
+    useful = sum(r[-1][0] // 8 for r in batched.values())
+    return {
+        "workload": "config 4: 64 searches, seeds LE32(j), 1..5000 prefixes (log-uniform) of 4..7 symbols, "
+        "quota 1..16; searches with expected work <= %.0e candidates" % cap,
+        "searches": len(searches),
+        "searches_in_config": len(all_searches),
+        "expected_candidates": sum(s.expected_candidates() for s in searches),
+        "candidates_to_quota": useful,
+        "results_identical": plain == batched,
+        "plain": {"wall_s": plain_wall, "examined": plain_examined, "keys_per_s": useful / plain_wall,
+                  "examined_per_s": plain_examined / plain_wall, "gpu_launches": plain_launches},
+        "batched": {"wall_s": batched_wall, "examined": examined, "keys_per_s": useful / batched_wall,
+                    "examined_per_s": examined / batched_wall, "device_s": dev_ms / 1e3, "steps": steps,
+                    "gpu_launches": launches},
+        "speedup_batched_over_plain": plain_wall / batched_wall,
+        "unit": "keys/s (candidates up to each search's quota-th hit, wall clock)",
+    }
+
+
+def serving_leg(dev, half, n, cap_s):
+    """Config 5: requests submitted at their Poisson arrival times."""
+    from onion_gen_b200 import serve, workloads
+
+    reqs = workloads.config5_requests(n)
+    s = serve.Server(dev, half=half)
+    t0 = s.now_ns()
+    submitted = 0
+    done = {}
+    while True:
+        now = (s.now_ns() - t0) / 1e9
+        while submitted < n and reqs[submitted].arrival <= now:
+            r = reqs[submitted]
+            s.submit(r.index, r.seed, r.prefixes, r.quota)
+            submitted += 1
+        for d in s.poll():
+            done[d.request_id] = d
+        if len(done) == n or now > cap_s:
+            break
+        time.sleep(0.002)
+    elapsed = (s.now_ns() - t0) / 1e9
+    st = s.stats()
+    s.close()
+    ok = [d for d in done.values() if d.status == 0]
+    ttf = sorted((d.done_ns - d.arrival_ns) / 1e9 for d in ok)
+
+    def q(p):
+        return ttf[min(len(ttf) - 1, int(p * len(ttf)))] if ttf else None
+
+    return {
+        "workload": f"config 5: first {n} of 2000 requests, Poisson arrivals at 50/s (splitmix64(5)), "
+        "1..200 prefixes (log-uniform) of 4..7 symbols, quota 1..16",
+        "submitted": submitted,
+        "completed": len(ok),
+        "wall_cap_s": cap_s,
+        "elapsed_s": elapsed,
+        "p50_ttf_s": q(0.50),
+        "p99_ttf_s": q(0.99),
+        "ttf_note": "over the requests completed within the cap; the mix's total expected work exceeds what "
+        "one GPU examines in the cap, so the longest requests are still running when it ends",
+        "keys_per_s": st.candidates / elapsed,
+        "device_busy": st.device_ms / 1e3 / elapsed,
+        "steps": int(st.steps),
+    }
+
+
 def pp_per_candidate(half):
     """Partial products per candidate of the paired round: (21 + 10 half)
     multiplications of 64 and 254 squarings of 36, over 2 half + 1 keys."""
@@ -317,10 +432,10 @@ def main():
             for _ in range(advances):
                 o, k = e.advance_raw()
                 d2h += 4 + 48 * len(o)
-                for off, packed in zip(o, k):
-                    if fs.match_key(bytes(packed)) is not None:
-                        key.check_hit(seed, int(off) + (rank << 43), bytes(packed))
-                        hits += 1
+                matched = fs.match_many(k)
+                for j in np.nonzero(matched >= 0)[0]:
+                    key.check_hit(seed, int(o[j]) + (rank << 43), bytes(k[j]))
+                    hits += 1
             e.close()
         barrier()
         e2e_wall = time.perf_counter() - t1
@@ -378,6 +493,14 @@ def main():
         if e2e:
             line["e2e"] = e2e
         line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+        if args.suite in ("default", "batched"):
+            cap = args.batched_cap if args.suite == "default" else float("inf")
+            line["batched"] = batched_leg(dev, args.half, cap)
+            line["gpu_launches"] += line["batched"]["batched"]["gpu_launches"] + line["batched"]["plain"]["gpu_launches"]
+        if args.suite in ("default", "serving"):
+            n = args.serving_requests if args.suite == "default" else 2000
+            cap = args.serving_cap if args.suite == "default" else 120.0
+            line["serving"] = serving_leg(dev, args.half, n, cap)
         print(json.dumps(line), flush=True)
     if pg:
         pg.destroy_process_group()

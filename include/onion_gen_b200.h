@@ -332,6 +332,10 @@ size_t og_filters_words(const og_filters* f, const uint64_t** words);
 double og_filters_occupancy(const og_filters* f);
 /* FilterSet::match_key (src/filter.rs:2098): index of the match or -1. */
 long og_filters_match(const og_filters* f, const uint8_t packed[32]);
+/* match_key over `n` keys laid out `stride` bytes apart (a survivor array's
+ * packed fields): writes each key's match or -1 to `out`, returns the number
+ * that matched. */
+size_t og_filters_match_many(const og_filters* f, const uint8_t* packed, size_t n, size_t stride, int32_t* out);
 void og_filters_free(og_filters* f);
 
 #ifdef __cplusplus

@@ -286,9 +286,9 @@ void release_blocks(og_batch* b, Search& s) {
 }
 
 // Shares the slot pool equally among unfinished searches (the earliest
-// admitted first when there are more searches than blocks). Searches above
-// their share drop their highest blocks; those below take free blocks, whose
-// lanes are queued for initialisation.
+// admitted first when there are more searches than blocks). Searches well
+// above their share drop their highest blocks; those below take free
+// blocks, whose lanes are queued for initialisation.
 void rebalance(og_batch* b, std::vector<uint32_t>& init) {
     std::vector<Search*> running;
     for (auto& kv : b->searches)
@@ -298,8 +298,13 @@ void rebalance(og_batch* b, std::vector<uint32_t>& init) {
     std::vector<uint32_t> target(running.size(), 0);
     for (size_t i = 0; i < n_sched; i++)
         target[i] = (uint32_t)(b->nblocks / n_sched + (i < b->nblocks % n_sched ? 1 : 0));
+    // Shrink only searches well above their share (a quarter over, at least
+    // one block), so that arrivals and departures do not reshuffle every
+    // search by a block each time; the free blocks go to those below it.
     for (size_t i = 0; i < running.size(); i++) {
         Search& s = *running[i];
+        const size_t slack = target[i] ? std::max<size_t>(1, target[i] / 4) : 0;
+        if (s.blocks.size() <= target[i] + slack) continue;
         while (s.blocks.size() > target[i]) {
             b->free_blocks.push_back(s.blocks.back());
             s.blocks.pop_back();

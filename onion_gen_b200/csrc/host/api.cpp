@@ -103,6 +103,17 @@ double og_filters_occupancy(const og_filters* f) { return f ? f->set.occupancy()
 
 long og_filters_match(const og_filters* f, const uint8_t packed[32]) { return f ? f->set.match_key(packed) : -1; }
 
+size_t og_filters_match_many(const og_filters* f, const uint8_t* packed, size_t n, size_t stride, int32_t* out) {
+    if (!f || !packed || !out) return 0;
+    size_t hits = 0;
+    for (size_t i = 0; i < n; i++) {
+        const long m = f->set.match_key(packed + i * stride);
+        out[i] = (int32_t)m;
+        if (m >= 0) hits++;
+    }
+    return hits;
+}
+
 void og_filters_free(og_filters* f) { delete f; }
 
 }  // extern "C"

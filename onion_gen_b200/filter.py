@@ -57,6 +57,14 @@ class FilterSet:
     def occupancy(self) -> float:
         return N.lib.og_filters_occupancy(self._h)
 
+    def match_many(self, packed) -> np.ndarray:
+        """match_key over an (n, 32) uint8 array: int32 indices, -1 where none matches."""
+        arr = np.ascontiguousarray(packed, dtype=np.uint8)
+        out = np.empty(len(arr), dtype=np.int32)
+        if len(arr):
+            N.lib.og_filters_match_many(self._h, arr.ctypes.data, len(arr), arr.strides[0], out.ctypes.data)
+        return out
+
     def match_key(self, packed: bytes):
         """Index of the filter this packed key matches, or None."""
         i = N.lib.og_filters_match(self._h, bytes(packed))

@@ -12,6 +12,8 @@ from __future__ import annotations
 
 from dataclasses import dataclass
 
+import numpy as np
+
 from . import filter as F
 from . import gpu, key
 
@@ -39,16 +41,14 @@ def device_search(device, seed: bytes, prefixes, quota: int, threads: int = 0, c
             offsets, packed = eng.advance_raw()
             advances += 1
             examined += eng.batch()
-            for off, p in zip(offsets, packed):
-                b = bytes(p)
-                f = fs.match_key(b)
-                if f is None:
-                    continue  # the bitmap said maybe, the exact check said no
-                pk, _ = key.check_hit(seed, int(off), b)
+            matched = fs.match_many(packed)  # the bitmap says maybe, the exact check decides
+            for j in np.nonzero(matched >= 0)[0]:
+                off, b, f = int(offsets[j]), bytes(packed[j]), int(matched[j])
+                pk, _ = key.check_hit(seed, off, b)
                 text = fs.texts()[f]
                 if len(text) > 49 and not key.address(pk).startswith(text):
                     continue
-                found.append(Found(int(off), b, pk, f))
+                found.append(Found(off, b, pk, f))
     finally:
         eng.close()
     found.sort(key=lambda h: h.offset)

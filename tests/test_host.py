@@ -151,3 +151,15 @@ def test_index_never_loses_a_match(native, oracle):
         packed[: nb - 1] = raw[: nb - 1]
         packed[nb - 1] = (noise[nb - 1] & ~mask & 0xFF) | (raw[nb - 1] & mask)
         assert fs.match_key(bytes(packed)) == texts.index(t)
+
+
+def test_match_many_agrees_with_match_key(native):
+    import numpy as np
+
+    fs = native.filter.FilterSet.parse_all(["abc", "q7", "zz2a"])
+    rng = np.random.default_rng(3)
+    keys = rng.integers(0, 256, size=(5000, 32), dtype=np.uint8)
+    keys[::7, :2] = np.frombuffer(bytes.fromhex("00a1"), dtype=np.uint8)  # 'ab' + bits
+    got = fs.match_many(keys)
+    want = [fs.match_key(bytes(k)) for k in keys]
+    assert [(-1 if w is None else w) for w in want] == got.tolist()

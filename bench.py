@@ -496,7 +496,6 @@ def main():
         if args.suite in ("default", "batched"):
             cap = args.batched_cap if args.suite == "default" else float("inf")
             line["batched"] = batched_leg(dev, args.half, cap)
-            line["gpu_launches"] += line["batched"]["batched"]["gpu_launches"] + line["batched"]["plain"]["gpu_launches"]
         if args.suite in ("default", "serving"):
             n = args.serving_requests if args.suite == "default" else 2000
             cap = args.serving_cap if args.suite == "default" else 120.0

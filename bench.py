@@ -204,6 +204,10 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def log(msg):
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
+
+
 def batched_leg(dev, half, cap):
     """Config 4: plain (one engine per search) against batched, same searches."""
     from onion_gen_b200 import _native as N
@@ -221,6 +225,7 @@ def batched_leg(dev, half, cap):
         plain_examined += examined
         plain_launches += 2 * advances + 1
     plain_wall = time.perf_counter() - t0
+    log(f"batched leg: plain engine {len(searches)} searches in {plain_wall:.2f} s")
 
     t0 = time.perf_counter()
     b = B.Batch(dev, half=half)
@@ -238,6 +243,7 @@ def batched_leg(dev, half, cap):
     batched = {s.index: [(h.offset, h.packed) for h in b.results(s.index)] for s in searches}
     b.close()
     batched_wall = time.perf_counter() - t0
+    log(f"batched leg: batched engine in {batched_wall:.2f} s, {steps} steps")
     useful = sum(r[-1][0] // 8 for r in batched.values())
     return {
         "workload": "config 4: 64 searches, seeds LE32(j), 1..5000 prefixes (log-uniform) of 4..7 symbols, "
@@ -278,6 +284,7 @@ def serving_leg(dev, half, n, cap_s):
             break
         time.sleep(0.002)
     elapsed = (s.now_ns() - t0) / 1e9
+    log(f"serving leg: {len(done)} of {submitted} done in {elapsed:.1f} s")
     st = s.stats()
     s.close()
     ok = [d for d in done.values() if d.status == 0]
@@ -400,6 +407,7 @@ def main():
             survivors += s
         barrier()
         wall = time.perf_counter() - t0
+    log(f"plain line: {sum(dev_ms):.1f} ms device time over {args.steps} steps")
     total_ms = sum(dev_ms)
     per_rank = np.array([total_ms, wall], dtype=np.float64)
     if pg:

@@ -31,6 +31,7 @@ def device_search(device, seed: bytes, prefixes, quota: int, threads: int = 0, c
     words, bits = fs.index_words()
     start = key.start_point(seed)
     eng = gpu.Engine(device, start, threads=threads, bitmap=words, bitmap_bits=bits, config=config)
+    texts = fs.texts()
     found = []
     advances = 0
     examined = 0
@@ -42,13 +43,17 @@ def device_search(device, seed: bytes, prefixes, quota: int, threads: int = 0, c
             advances += 1
             examined += eng.batch()
             matched = fs.match_many(packed)  # the bitmap says maybe, the exact check decides
-            for j in np.nonzero(matched >= 0)[0]:
+            idx = np.nonzero(matched >= 0)[0]
+            # this advance's range lies above every earlier one: its matches
+            # in offset order are the next hits, up to the quota
+            for j in idx[np.argsort(offsets[idx], kind="stable")]:
                 off, b, f = int(offsets[j]), bytes(packed[j]), int(matched[j])
                 pk, _ = key.check_hit(seed, off, b)
-                text = fs.texts()[f]
-                if len(text) > 49 and not key.address(pk).startswith(text):
+                if len(texts[f]) > 49 and not key.address(pk).startswith(texts[f]):
                     continue
                 found.append(Found(off, b, pk, f))
+                if len(found) == quota:
+                    break
     finally:
         eng.close()
     found.sort(key=lambda h: h.offset)

@@ -60,8 +60,9 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--case", default="full", choices=["full", "small"],
-                   help="small: the profiling case, three one-round advances of the plain engine")
+    p.add_argument("--case", default="full", choices=["full", "small", "batch-small"],
+                   help="small: the profiling case, three one-round advances of the plain engine; "
+                   "batch-small: three steps of the batched engine over the first 16 config-4 searches")
     p.add_argument("--half", type=int, default=HALF)
     p.add_argument("--suite", default="default", choices=["default", "batched", "serving", "plain"],
                    help="default: the plain line plus bounded batched and serving legs; "
@@ -334,6 +335,23 @@ def small_case(args):
         print(f"advance {i}: {len(o)} survivors, kernel {ms:.3f} ms, {eng.batch() / ms * 1e3:.4e} keys/s")
 
 
+def batch_small_case(args):
+    """Three steps of the batched engine with the first 16 config-4 searches
+    admitted: the case the batched kernels' ncu summaries are captured on."""
+    from onion_gen_b200 import batch as B
+    from onion_gen_b200 import gpu, workloads
+
+    dev = gpu.look()[0]
+    b = B.Batch(dev, half=args.half)
+    for s in workloads.config4_searches()[:16]:
+        b.admit(s.index, s.seed, s.prefixes, s.quota)
+    for i in range(3):
+        b.step()
+        ms = b.last_step_ms()
+        print(f"step {i}: {b.last_step_candidates()} candidates, {ms:.3f} ms, "
+              f"{b.last_step_candidates() / ms * 1e3:.4e} keys/s, running {b.running()}")
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -341,6 +359,9 @@ def main():
         return
     if args.case == "small":
         small_case(args)
+        return
+    if args.case == "batch-small":
+        batch_small_case(args)
         return
     rank, world, local = dist_env()
     import ctypes as C

@@ -50,6 +50,12 @@ sys.path.insert(0, ROOT)
 CANDIDATES_PER_STEP = 1 << 32
 HALF = 256
 CPU_HALF = 4096  # PairEngine::new(8192) (src/run.rs:601, src/batch.rs:32)
+# DRAM bytes per candidate of paired_kernel at half 256, from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum = 15.01 GB for 116,619,264
+# candidates); the algorithmic figure is 128 B (the Montgomery scratch, 64 B
+# written and 64 B read per candidate).
+TRAFFIC_PER_CANDIDATE = 128.7
+ALGORITHMIC_BYTES_PER_CANDIDATE = 128
 
 
 def parse():
@@ -445,6 +451,11 @@ def main():
     err = N.errbuf()
     N.check(N.lib.og_measure_int_peak(dev.ordinal, C.byref(imad), C.byref(mulpp), err, 512), err)
     w = pp_per_candidate(shape.half)
+    hbm_peak = None
+    try:
+        hbm_peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+    except (OSError, KeyError, ValueError):
+        hbm_peak = 6650.0  # the pool's earlier measurement, when the driver's file is absent
     achieved = value / world * w
     peak = imad.value / 2.0
 
@@ -512,10 +523,18 @@ def main():
                 "peak": peak,
                 "unit": "partial products/s",
                 "frac": achieved / peak,
-                "traffic": None,
+                "traffic": TRAFFIC_PER_CANDIDATE * batch if args.half == 256 else None,
+                "traffic_unit": "DRAM bytes per launch (ncu, dram__bytes_read.sum + dram__bytes_write.sum)",
                 "per_candidate": w,
                 "peak_source": "measured: og_measure_int_peak mad.lo.u32 issue rate / 2 (lo+hi per product)",
                 "fe_mul_pp_per_s": mulpp.value,
+                "hbm": {
+                    "achieved": value / world * ALGORITHMIC_BYTES_PER_CANDIDATE / 1e9,
+                    "peak": hbm_peak,
+                    "unit": "GB/s",
+                    "frac": value / world * ALGORITHMIC_BYTES_PER_CANDIDATE / 1e9 / hbm_peak if hbm_peak else None,
+                    "note": "the Montgomery scratch: not the bound",
+                },
             },
             "clocks": clocks.summary(),
         }

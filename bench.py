@@ -377,7 +377,7 @@ def main():
 
     from onion_gen_b200 import _native as N
     from onion_gen_b200 import filter as F
-    from onion_gen_b200 import gpu, key, workloads
+    from onion_gen_b200 import gpu, key, shard, workloads
 
     torch.cuda.set_device(local)
     pg = None
@@ -399,10 +399,8 @@ def main():
     prefix = workloads.config2_prefix()
     fs = F.FilterSet.parse_all([prefix])
     words, bits = fs.index_words()
-    # rank r searches offsets [r * 2^40 * 8, ...): start = s B + r 2^43 B
-    # rank r searches its own range: base scalar s + r 2^43 (offsets below 2^43 never meet)
-    scalar = int.from_bytes(key.secret_scalar(seed), "little") + (rank << 43)
-    base = key.scalar_base_mult(scalar.to_bytes(32, "little"))
+    # rank r searches its own range of offsets (shard.RANK_SHIFT apart)
+    base = shard.rank_start(seed, rank)
 
     cfg = N.EngineConfig(N.SCHEME_PAIRED, args.half, 0, 0, 128, 0, 0)
     eng = gpu.Engine(dev, base, bitmap=words, bitmap_bits=bits, config=cfg)
@@ -435,13 +433,7 @@ def main():
         barrier()
         wall = time.perf_counter() - t0
     log(f"plain line: {sum(dev_ms):.1f} ms device time over {args.steps} steps")
-    total_ms = sum(dev_ms)
-    per_rank = np.array([total_ms, wall], dtype=np.float64)
-    if pg:
-        t = torch.tensor(per_rank, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        per_rank = t.cpu().numpy()
-    total_ms, wall = float(per_rank[0]), float(per_rank[1])
+    total_ms, wall = shard.max_over_ranks([sum(dev_ms), wall])
     keys = batch * advances * args.steps * world
     value = keys / (total_ms * 1e-3)
 
@@ -474,7 +466,7 @@ def main():
                 d2h += 4 + 48 * len(o)
                 matched = fs.match_many(k)
                 for j in np.nonzero(matched >= 0)[0]:
-                    key.check_hit(seed, int(o[j]) + (rank << 43), bytes(k[j]))
+                    key.check_hit(seed, shard.global_offset(rank, int(o[j])), bytes(k[j]))
                     hits += 1
             e.close()
         barrier()

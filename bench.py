@@ -48,12 +48,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 CANDIDATES_PER_STEP = 1 << 32
-HALF = 256
+HALF = 1024
+# the batched engine keeps rounds short: a step is one round of every lane
+BATCH_HALF = 256
 CPU_HALF = 4096  # PairEngine::new(8192) (src/run.rs:601, src/batch.rs:32)
-# DRAM bytes per candidate of paired_kernel at half 256, from one ncu capture
+# DRAM bytes per candidate of paired_kernel, from one ncu capture at half 256
 # (dram__bytes_read.sum + dram__bytes_write.sum = 15.01 GB for 116,619,264
 # candidates); the algorithmic figure is 128 B (the Montgomery scratch, 64 B
-# written and 64 B read per candidate).
+# written and 64 B read per candidate) whatever the half.
 TRAFFIC_PER_CANDIDATE = 128.7
 ALGORITHMIC_BYTES_PER_CANDIDATE = 128
 
@@ -515,7 +517,7 @@ def main():
                 "peak": peak,
                 "unit": "partial products/s",
                 "frac": achieved / peak,
-                "traffic": TRAFFIC_PER_CANDIDATE * batch if args.half == 256 else None,
+                "traffic": TRAFFIC_PER_CANDIDATE * batch,
                 "traffic_unit": "DRAM bytes per launch (ncu, dram__bytes_read.sum + dram__bytes_write.sum)",
                 "per_candidate": w,
                 "peak_source": "measured: og_measure_int_peak mad.lo.u32 issue rate / 2 (lo+hi per product)",
@@ -535,11 +537,11 @@ def main():
         line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
         if args.suite in ("default", "batched"):
             cap = args.batched_cap if args.suite == "default" else float("inf")
-            line["batched"] = batched_leg(dev, args.half, cap)
+            line["batched"] = batched_leg(dev, BATCH_HALF, cap)
         if args.suite in ("default", "serving"):
             n = args.serving_requests if args.suite == "default" else 2000
             cap = args.serving_cap if args.suite == "default" else 120.0
-            line["serving"] = serving_leg(dev, args.half, n, cap)
+            line["serving"] = serving_leg(dev, BATCH_HALF, n, cap)
         print(json.dumps(line), flush=True)
     if pg:
         pg.destroy_process_group()

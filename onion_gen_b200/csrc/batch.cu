@@ -123,9 +123,8 @@ __global__ void __launch_bounds__(BLOCK) batch_init_kernel(const BatchArgs a) {
 // pool is exhausted. Every block of lanes belongs to one search, whose
 // descriptor gives its stride and bitmap.
 __global__ void __launch_bounds__(OG_LB_THREADS, OG_LB_MIN_BLOCKS) batch_search_kernel(const BatchArgs a) {
-    extern __shared__ uint4 qtab[];
+    const uint4* qtab = a.table;  // read through L1, as the single-search kernel does
     __shared__ uint32_t item_s;
-    for (uint32_t i = threadIdx.x; i < a.half * 6; i += blockDim.x) qtab[i] = a.table[i];
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) item_s = atomicAdd(&a.counters->work, 1u);
@@ -370,9 +369,7 @@ int og_batch_new(int ordinal, const og_batch_config* cfgp, og_batch** out, char*
     std::unique_ptr<og_batch> b(new (std::nothrow) og_batch());
     if (!b) return fail(err, errlen, OG_E_NOMEM, "host memory");
     b->device = ordinal;
-    b->smem = (size_t)cfg.half * 96;
-    if (b->smem > 48 * 1024)
-        CU(cudaFuncSetAttribute(batch_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+    b->smem = 0;
     int per_sm = 0, sms = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_search_kernel, BLOCK, b->smem));
     CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ordinal));

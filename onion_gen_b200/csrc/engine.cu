@@ -183,7 +183,7 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
     if (cfg.block == 0) cfg.block = 128;
     if (cfg.block % 32 || cfg.block > OG_LB_THREADS)
         return fail(err, errlen, OG_E_ARG, "block %u (a multiple of 32, at most %d)", cfg.block, OG_LB_THREADS);
-    if (cfg.half == 0) cfg.half = 256;
+    if (cfg.half == 0) cfg.half = 1024;
     if (cfg.scheme == OG_SCHEME_PAIRED && cfg.half > 2048) return fail(err, errlen, OG_E_ARG, "half %u > 2048", cfg.half);
     if (cfg.scheme == OG_SCHEME_CHAIN && cfg.half > 65536) return fail(err, errlen, OG_E_ARG, "n %u > 65536", cfg.half);
     if (cfg.lanes == 0) {
@@ -387,7 +387,7 @@ int og_engine_new(int ordinal, const uint8_t start[128], uint32_t threads, const
     og_engine* best = nullptr;
     double best_rate = -1;
     int last = OG_E_DEVICE;
-    for (uint32_t half : {128u, 256u, 512u}) {
+    for (uint32_t half : {256u, 512u, 1024u}) {
         uint32_t resident = 0;
         if (resident_lanes(ordinal, OG_SCHEME_PAIRED, half, 128, &resident, err, errlen) != OG_OK) continue;
         for (uint32_t mult : {1u, 2u, 3u}) {

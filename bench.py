@@ -10,10 +10,11 @@ candidates actually examined are what is counted). Inputs are synthetic.
 One JSON line on rank 0:
   value       keys/s over the timed steps, device time (CUDA events on the
               engine's stream around every kernel launch), max over ranks
-  e2e         keys/s through the C ABI as a caller uses it: engine creation
-              (host precompute, H2D of the start point, tables and bitmap),
-              every advance (D2H of the survivors) and the host's exact match
-              and independent re-derivation of every hit, wall clock
+  e2e         keys/s through the C ABI as a caller uses it: one engine for
+              the run, its creation (host precompute, H2D of the start point,
+              tables and bitmap) and free, every advance (D2H of the
+              survivors) and the host's exact match and independent
+              re-derivation of every hit, wall clock
   roofline    integer-multiply bound: partial products/s achieved by the
               search kernel against the measured multiply-add issue rate
   cpu_baseline the oracle's restatement of the reference's paired CPU engine
@@ -71,7 +72,9 @@ def parse():
     p.add_argument("--case", default="full", choices=["full", "small", "batch-small"],
                    help="small: the profiling case, three one-round advances of the plain engine; "
                    "batch-small: three steps of the batched engine over the first 16 config-4 searches")
-    p.add_argument("--half", type=int, default=HALF)
+    p.add_argument("--half", type=int, default=0,
+                   help=f"inversion batch half-width (default {HALF} for the plain line, 256 for --case small, "
+                   f"{BATCH_HALF} for the batched engine)")
     p.add_argument("--suite", default="default", choices=["default", "batched", "serving", "plain"],
                    help="default: the plain line plus bounded batched and serving legs; "
                    "batched / serving: that leg at full size; plain: the plain line only")
@@ -326,21 +329,27 @@ def pp_per_candidate(half):
 
 
 def small_case(args):
-    """Three advances of one round each at the default shape: the case the
-    ncu summaries under profiles/ are captured on (about 1.6 GB of scratch)."""
+    """Three advances of one round each: the case the ncu summaries under
+    profiles/ are captured on. Half 256 (or --half) and one resident wave of
+    lanes (SMs x 6 blocks x 128) keep the scratch near 3.8 GB; the kernel is
+    the production one, and its DRAM bytes per candidate do not depend on the
+    shape (64 B written and read back per candidate)."""
     from onion_gen_b200 import _native as N
     from onion_gen_b200 import filter as F
     from onion_gen_b200 import gpu, key, workloads
 
     dev = gpu.look()[0]
+    half = args.half or 256
+    lanes = dev.sms * 6 * 128
     fs = F.FilterSet.parse_all([workloads.config2_prefix()])
     words, bits = fs.index_words()
     start = key.start_point(workloads.seed(0))
-    eng = gpu.Engine(dev, start, bitmap=words, bitmap_bits=bits, config=N.EngineConfig(0, args.half, 0, 1, 128, 0, 0))
+    eng = gpu.Engine(dev, start, bitmap=words, bitmap_bits=bits, config=N.EngineConfig(0, half, lanes, 1, 128, 0, 0))
     for i in range(3):
         o, _ = eng.advance_raw()
         ms = eng.last_kernel_ms()
-        print(f"advance {i}: {len(o)} survivors, kernel {ms:.3f} ms, {eng.batch() / ms * 1e3:.4e} keys/s")
+        print(f"advance {i}: half {half}, {lanes} lanes, {len(o)} survivors, kernel {ms:.3f} ms, "
+              f"{eng.batch() / ms * 1e3:.4e} keys/s")
 
 
 def batch_small_case(args):
@@ -350,7 +359,7 @@ def batch_small_case(args):
     from onion_gen_b200 import gpu, workloads
 
     dev = gpu.look()[0]
-    b = B.Batch(dev, half=args.half)
+    b = B.Batch(dev, half=args.half or BATCH_HALF)
     for s in workloads.config4_searches()[:16]:
         b.admit(s.index, s.seed, s.prefixes, s.quota)
     for i in range(3):
@@ -404,7 +413,7 @@ def main():
     # rank r searches its own range of offsets (shard.RANK_SHIFT apart)
     base = shard.rank_start(seed, rank)
 
-    cfg = N.EngineConfig(N.SCHEME_PAIRED, args.half, 0, 0, 128, 0, 0)
+    cfg = N.EngineConfig(N.SCHEME_PAIRED, args.half or HALF, 0, 0, 128, 0, 0)
     eng = gpu.Engine(dev, base, bitmap=words, bitmap_bits=bits, config=cfg)
     shape = eng.shape()
     batch = eng.batch()
@@ -453,16 +462,22 @@ def main():
     achieved = value / world * w
     peak = imad.value / 2.0
 
-    # end to end through the C ABI, host buffers, every hit re-derived
+    # end to end through the C ABI, host buffers, every hit re-derived. As
+    # the reference's device worker (src/run.rs:1030-1119) does, one engine
+    # serves the whole run: it is created (host precompute, H2D of the start
+    # point, tables and bitmap) and freed inside the timed region, and every
+    # step is `advances` advances with the D2H of their survivors.
     e2e = None
     if not args.no_e2e:
         h2d = d2h = 0
         hits = 0
+        e2e_steps = args.steps
         barrier()
         t1 = time.perf_counter()
-        for _ in range(max(1, args.steps // 2)):
-            e = gpu.Engine(dev, base, bitmap=words, bitmap_bits=bits, config=cfg)
-            h2d += 128 + words.nbytes + shape.half * 96
+        e = gpu.Engine(dev, base, bitmap=words, bitmap_bits=bits, config=cfg)
+        h2d += 128 + words.nbytes + shape.half * 96
+        t_created = time.perf_counter()
+        for _ in range(e2e_steps):
             for _ in range(advances):
                 o, k = e.advance_raw()
                 d2h += 4 + 48 * len(o)
@@ -470,10 +485,10 @@ def main():
                 for j in np.nonzero(matched >= 0)[0]:
                     key.check_hit(seed, shard.global_offset(rank, int(o[j])), bytes(k[j]))
                     hits += 1
-            e.close()
+        t_advanced = time.perf_counter()
+        e.close()
         barrier()
         e2e_wall = time.perf_counter() - t1
-        e2e_steps = max(1, args.steps // 2)
         e2e = {
             "value": batch * advances * e2e_steps * world / e2e_wall,
             "unit": "keys/s",
@@ -481,7 +496,11 @@ def main():
             "d2h_bytes_per_step": d2h // e2e_steps,
             "steps": e2e_steps,
             "hits_verified": hits,
+            "engine_create_s": t_created - t1,
+            "engine_free_s": e2e_wall - (t_advanced - t1),
         }
+        log(f"e2e: create {t_created - t1:.3f} s, {e2e_steps} steps {t_advanced - t_created:.3f} s, "
+            f"free {e2e_wall - (t_advanced - t1):.3f} s")
 
     if rank == 0:
         line = {

@@ -53,11 +53,12 @@ HALF = 1024
 # the batched engine keeps rounds short: a step is one round of every lane
 BATCH_HALF = 256
 CPU_HALF = 4096  # PairEngine::new(8192) (src/run.rs:601, src/batch.rs:32)
-# DRAM bytes per candidate of paired_kernel, from one ncu capture at half 256
-# (dram__bytes_read.sum + dram__bytes_write.sum = 15.01 GB for 116,619,264
-# candidates); the algorithmic figure is 128 B (the Montgomery scratch, 64 B
-# written and 64 B read per candidate) whatever the half.
-TRAFFIC_PER_CANDIDATE = 128.7
+# DRAM bytes per candidate of paired_kernel, from one ncu capture of one
+# launch at the plain line's shape (half 1024, 227,328 lanes:
+# dram__bytes_read.sum + dram__bytes_write.sum = 29.95 + 29.91 GB for
+# 465,795,072 candidates); the algorithmic figure is 128 B (the Montgomery
+# scratch, 64 B written and 64 B read per candidate) whatever the half.
+TRAFFIC_PER_CANDIDATE = 128.5
 ALGORITHMIC_BYTES_PER_CANDIDATE = 128
 
 

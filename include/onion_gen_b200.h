@@ -113,6 +113,37 @@ int og_engine_advance(og_engine* e, og_survivor* out, size_t cap, size_t* n, cha
  * engine's stream). */
 float og_engine_last_kernel_ms(const og_engine* e);
 
+/* ---- device-side exact match for the engine ------------------------------
+ *
+ * FilterSet::match_key (src/filter.rs:2194-2213, with the length buckets of
+ * :2645-2700), which the reference runs on the host for every survivor
+ * (run::device_worker, src/run.rs:1081-1085), moved onto the device: the
+ * bitmap survivors of an advance are matched there and only exact matches
+ * cross back. */
+
+/* One exact match: the survivor and the index of the filter it matches in
+ * the filter set's kept order (og_filters_text). */
+typedef struct og_match {
+    uint64_t offset;    /* scalar delta from the start, as og_survivor */
+    uint8_t packed[32]; /* canonical y, sign bit cleared */
+    uint32_t filter;
+    uint32_t pad;
+} og_match;
+
+/* Turns the device match on. `f` must be the filter set whose index_words the
+ * engine was created with (same width and the same bitmap, checked:
+ * OG_E_ARG otherwise); its exact-match tables are copied and `f` is not
+ * referenced afterwards. An engine created with dump = 1 has no bitmap and
+ * refuses (OG_E_STATE). */
+int og_engine_match_on_device(og_engine* e, const struct og_filters* f, char* err, size_t errlen);
+
+/* One advance that returns only the exact matches (room `cap`, count `*n`).
+ * Survivors beyond the engine's room are OG_E_OVERFLOW as in
+ * og_engine_advance. Filters longer than 12 symbols are matched on their
+ * first 12 on the device and confirmed on the host before they are
+ * returned. */
+int og_engine_advance_matches(og_engine* e, og_match* out, size_t cap, size_t* n, char* err, size_t errlen);
+
 void og_engine_free(og_engine* e);
 
 /* ---- the batched engine: many searches in one persistent kernel ---------

@@ -42,6 +42,10 @@ class Survivor(C.Structure):
     _fields_ = [("offset", C.c_uint64), ("packed", C.c_uint8 * 32)]
 
 
+class Match(C.Structure):
+    _fields_ = [("offset", C.c_uint64), ("packed", C.c_uint8 * 32), ("filter", C.c_uint32), ("pad", C.c_uint32)]
+
+
 class EngineConfig(C.Structure):
     _fields_ = [
         ("scheme", C.c_uint32),
@@ -145,6 +149,8 @@ def _load():
     sig("og_engine_shape", None, [P, C.POINTER(EngineConfig)])
     sig("og_engine_advance", I, [P, P, SZ, C.POINTER(SZ), B, SZ])
     sig("og_engine_last_kernel_ms", C.c_float, [P])
+    sig("og_engine_match_on_device", I, [P, P, B, SZ])
+    sig("og_engine_advance_matches", I, [P, P, SZ, C.POINTER(SZ), B, SZ])
     sig("og_engine_free", None, [P])
     sig("og_batch_new", I, [I, C.POINTER(BatchConfig), C.POINTER(P), B, SZ])
     sig("og_batch_admit", I, [P, U64, B, B, U32, B, SZ])

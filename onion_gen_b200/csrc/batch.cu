@@ -45,12 +45,14 @@ namespace og {
 
 const std::vector<uint4>& pair_table(uint32_t half);           // engine.cu
 std::vector<uint4> pow2_table(const Pt& stride, uint32_t nbits);  // engine.cu
+MatchTables match_tables(const std::vector<FilterSet::DeviceBucket>& buckets, const uint64_t* keys,
+                         const uint32_t* owners);                  // engine.cu
 
 namespace {
 
 constexpr uint32_t BLOCK = 128;
 constexpr uint32_t NONE = 0xffffffffu;
-constexpr int MAX_BUCKETS = 12;
+constexpr int MAX_BUCKETS = MAX_MATCH_BUCKETS;
 constexpr uint32_t POW2_BITS = 24;  // lanes of one search stay below 2^24
 // A filter set whose bitmap lets more than this fraction of candidates
 // through is refused: the survivor buffer is sized from it.
@@ -60,13 +62,8 @@ struct BatchDesc {
     FeWords wx, wy, wt;      // the search's stride for this step: L (2 half + 1) 8 G, affine
     FeWords bx, by, bz, bt;  // centre of window W_done (where new lanes start), extended
     const uint32_t* bitmap;
-    const uint64_t* keys;
-    const uint32_t* owners;
     uint32_t bits;
-    uint32_t nbuckets;
-    uint32_t bucket_bits[MAX_BUCKETS];
-    uint32_t bucket_off[MAX_BUCKETS];
-    uint32_t bucket_len[MAX_BUCKETS];
+    MatchTables match;
 };
 
 struct SlotBlock {
@@ -151,26 +148,13 @@ __global__ void __launch_bounds__(256) batch_exact_kernel(const BatchArgs a) {
     const uint32_t n = min(a.counters->surv, a.surv_cap);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const HitRec r = a.surv[i];
-        const BatchDesc& d = a.descs[r.search];
-        const uint64_t head =
-            ((uint64_t)__byte_perm(r.y[0], 0, 0x0123) << 32) | (uint64_t)__byte_perm(r.y[1], 0, 0x0123);
-        for (uint32_t b = 0; b < d.nbuckets; b++) {
-            const uint64_t probe = head & (~0ULL << (64 - d.bucket_bits[b]));
-            const uint64_t* k = d.keys + d.bucket_off[b];
-            uint32_t lo = 0, hi = d.bucket_len[b];
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (k[mid] < probe) lo = mid + 1;
-                else hi = mid;
-            }
-            if (lo < d.bucket_len[b] && k[lo] == probe) {
-                const uint32_t idx = atomicAdd(&a.counters->hits, 1u);
-                if (idx < a.hit_cap) {
-                    HitRec h = r;
-                    h.pad = d.owners[d.bucket_off[b] + lo];
-                    a.hits[idx] = h;
-                }
-                break;
+        const uint32_t owner = exact_owner(a.descs[r.search].match, r.y[0], r.y[1]);
+        if (owner != NONE) {
+            const uint32_t idx = atomicAdd(&a.counters->hits, 1u);
+            if (idx < a.hit_cap) {
+                HitRec h = r;
+                h.pad = owner;
+                a.hits[idx] = h;
             }
         }
     }
@@ -515,15 +499,8 @@ int og_batch_admit(og_batch* b, uint64_t search_id, const uint8_t seed[32], cons
     BatchDesc& d = b->h_descs.p[s->sidx];
     std::memset(&d, 0, sizeof d);
     d.bitmap = s->bitmap.p;
-    d.keys = s->keys.p;
-    d.owners = s->owners.p;
     d.bits = s->fs.bits();
-    d.nbuckets = (uint32_t)s->buckets.size();
-    for (size_t i = 0; i < s->buckets.size(); i++) {
-        d.bucket_bits[i] = s->buckets[i].bits;
-        d.bucket_off[i] = s->buckets[i].offset;
-        d.bucket_len[i] = s->buckets[i].count;
-    }
+    d.match = match_tables(s->buckets, s->keys.p, s->owners.p);
     b->mark(s->sidx);
     s->admit_order = b->admitted++;
     b->mem_used += s->table_bytes;

@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -100,6 +101,35 @@ uint32_t bits_for(uint64_t v) {
     return b;
 }
 
+MatchTables match_tables(const std::vector<FilterSet::DeviceBucket>& buckets, const uint64_t* keys,
+                         const uint32_t* owners) {
+    MatchTables t{};
+    t.keys = keys;
+    t.owners = owners;
+    t.nbuckets = (uint32_t)std::min<size_t>(buckets.size(), MAX_MATCH_BUCKETS);
+    for (uint32_t i = 0; i < t.nbuckets; i++) {
+        t.bucket_bits[i] = buckets[i].bits;
+        t.bucket_off[i] = buckets[i].offset;
+        t.bucket_len[i] = buckets[i].count;
+    }
+    return t;
+}
+
+// FNV-1a over the words of a bitmap: identifies the bitmap an engine was
+// built with, so that a filter set handed in later can be checked against it.
+uint64_t words_hash(const uint64_t* w, size_t n) {
+    uint64_t h = 0xcbf29ce484222325ULL;
+    for (size_t i = 0; i < n; i++) {
+        uint64_t v = w[i];
+        for (int k = 0; k < 8; k++) {
+            h ^= v & 0xff;
+            h *= 0x100000001b3ULL;
+            v >>= 8;
+        }
+    }
+    return h;
+}
+
 }  // namespace og
 
 struct og_engine {
@@ -120,6 +150,17 @@ struct og_engine {
     HostBuf<uint32_t> h_counter;
     PairedArgs pa{};
     ChainArgs ca{};
+    uint64_t bitmap_hash = 0;  // of the bitmap the engine was created with
+    // device exact match (og_engine_match_on_device)
+    bool matching = false;
+    bool long_filters = false;  // some filter is longer than the device tables reach
+    og::FilterSet fs;
+    DevBuf<uint64_t> mkeys;
+    DevBuf<uint32_t> mowners, mcount;
+    DevBuf<HitRec> matches;
+    HostBuf<HitRec> h_matches;
+    HostBuf<uint32_t> h_mcount;
+    MatchArgs ma{};
 
     ~og_engine() {
         if (stream) {
@@ -239,6 +280,7 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
         const size_t w32 = (size_t)(((1ULL << bits) + 31) / 32);
         CU(e->bitmap.alloc(std::max<size_t>(w32, 2)));
         CU(cudaMemcpyAsync(e->bitmap.p, bitmap, w32 * 4, cudaMemcpyHostToDevice, e->stream));
+        e->bitmap_hash = words_hash(bitmap, (size_t)(((1ULL << bits) + 63) / 64));
     }
 
     // lane start points
@@ -485,6 +527,118 @@ int og_engine_advance(og_engine* e, og_survivor* out, size_t cap, size_t* n, cha
         }
     }
     *n = found;
+    return OG_OK;
+}
+
+int og_engine_match_on_device(og_engine* e, const og_filters* f, char* err, size_t errlen) {
+    if (!e || !f) return fail(err, errlen, OG_E_ARG, "null argument");
+    if (e->cfg.dump) return fail(err, errlen, OG_E_STATE, "the engine keeps every candidate: it has no bitmap to match behind");
+    if (f->set.bits() != e->bits)
+        return fail(err, errlen, OG_E_ARG, "the filter set's index is %u bits wide and the engine's %u", f->set.bits(),
+                    e->bits);
+    const size_t nwords = (size_t)(((1ULL << e->bits) + 63) / 64);
+    if (f->set.words().size() < nwords || words_hash(f->set.words().data(), nwords) != e->bitmap_hash)
+        return fail(err, errlen, OG_E_ARG, "the filter set's bitmap is not the one the engine was created with");
+    std::vector<FilterSet::DeviceBucket> buckets;
+    std::vector<uint64_t> keys;
+    std::vector<uint32_t> owners;
+    f->set.device_tables(buckets, keys, owners);
+    if (buckets.size() > (size_t)MAX_MATCH_BUCKETS)
+        return fail(err, errlen, OG_E_FILTER, "more than %d filter lengths", MAX_MATCH_BUCKETS);
+    e->matching = false;
+    CU(cudaSetDevice(e->device));
+    CU(cudaStreamSynchronize(e->stream));
+    CU(e->mkeys.alloc(std::max<size_t>(keys.size(), 1)));
+    CU(e->mowners.alloc(std::max<size_t>(owners.size(), 1)));
+    if (!keys.empty()) {
+        CU(cudaMemcpyAsync(e->mkeys.p, keys.data(), keys.size() * 8, cudaMemcpyHostToDevice, e->stream));
+        CU(cudaMemcpyAsync(e->mowners.p, owners.data(), owners.size() * 4, cudaMemcpyHostToDevice, e->stream));
+    }
+    CU(e->mcount.alloc(1));
+    CU(e->h_mcount.alloc(1));
+    CU(e->matches.alloc(e->cap));
+    CU(e->h_matches.alloc(e->cap));
+    CU(cudaStreamSynchronize(e->stream));
+    e->fs = f->set;
+    e->long_filters = false;
+    for (size_t i = 0; i < e->fs.size(); i++)
+        if (e->fs.filter(i).text.size() > FilterSet::DEVICE_SYMBOLS) e->long_filters = true;
+    MatchArgs& m = e->ma;
+    m.surv = e->hits.p;
+    m.surv_count = e->counter.p;
+    m.surv_cap = (uint32_t)std::min<size_t>(e->cap, 0xffffffffu);
+    m.t = match_tables(buckets, e->mkeys.p, e->mowners.p);
+    m.out = e->matches.p;
+    m.out_count = e->mcount.p;
+    m.out_cap = m.surv_cap;
+    e->matching = true;
+    return OG_OK;
+}
+
+int og_engine_advance_matches(og_engine* e, og_match* out, size_t cap, size_t* n, char* err, size_t errlen) {
+    if (!e || !n) return fail(err, errlen, OG_E_ARG, "null argument");
+    *n = 0;
+    if (!e->matching) return fail(err, errlen, OG_E_STATE, "og_engine_match_on_device has not been called");
+    if (e->overflowed) return fail(err, errlen, OG_E_STATE, "an earlier advance overflowed; the engine is closed");
+    CU(cudaSetDevice(e->device));
+    CU(cudaMemsetAsync(e->counter.p, 0, sizeof(uint32_t), e->stream));
+    CU(cudaMemsetAsync(e->mcount.p, 0, sizeof(uint32_t), e->stream));
+    CU(cudaEventRecord(e->ev0, e->stream));
+    if (e->cfg.scheme == OG_SCHEME_PAIRED) {
+        CU(launch_paired(e->pa, (int)e->cfg.block, e->stream));
+    } else {
+        CU(launch_chain(e->ca, (int)e->cfg.block, e->stream));
+    }
+    CU(cudaEventRecord(e->ev1, e->stream));
+    int sms = 0;
+    CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device));
+    CU(launch_match(e->ma, std::max(sms, 1) * 4, e->stream));
+    CU(cudaMemcpyAsync(e->h_counter.p, e->counter.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream));
+    CU(cudaMemcpyAsync(e->h_mcount.p, e->mcount.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream));
+    CU(cudaStreamSynchronize(e->stream));
+    cudaEventElapsedTime(&e->last_ms, e->ev0, e->ev1);
+    const uint64_t launch = e->launches++;
+    const uint32_t found = *e->h_counter.p;
+    if (found > e->cap) {
+        e->overflowed = true;
+        return fail(err, errlen, OG_E_OVERFLOW,
+                    "one advance produced %u survivors and only %zu fit; the index is too narrow for what it "
+                    "is filtering: a wider index is the answer",
+                    found, e->cap);
+    }
+    const uint32_t matched = *e->h_mcount.p;  // at most `found`, so within the buffer
+    if (matched) {
+        CU(cudaMemcpyAsync(e->h_matches.p, e->matches.p, (size_t)matched * sizeof(HitRec), cudaMemcpyDeviceToHost,
+                           e->stream));
+        CU(cudaStreamSynchronize(e->stream));
+    }
+    const uint64_t L = e->cfg.lanes, slots = e->slots, R = e->cfg.rounds;
+    const bool paired = e->cfg.scheme == OG_SCHEME_PAIRED;
+    size_t k = 0;
+    for (uint32_t j = 0; j < matched; j++) {
+        const HitRec& h = e->h_matches.p[j];
+        og_match m;
+        std::memset(&m, 0, sizeof m);
+        for (int q = 0; q < 8; q++)
+            for (int b = 0; b < 4; b++) m.packed[4 * q + b] = (uint8_t)(h.y[q] >> (8 * b));
+        m.filter = h.pad;
+        // With filters longer than the device tables reach, several can share
+        // the 12 symbols the device compared: the host's match decides which
+        // (if any) matches.
+        if (e->long_filters) {
+            const long f = e->fs.match_key(m.packed);
+            if (f < 0) continue;
+            m.filter = (uint32_t)f;
+        }
+        if (k == cap)
+            return fail(err, errlen, OG_E_CAPACITY, "more than %zu matches and room for %zu in the caller's buffer",
+                        cap, cap);
+        const uint64_t r = h.step / slots, i = h.step % slots;
+        const uint64_t w = (launch * R + r) * L + h.lane;
+        m.offset = paired ? 8 * (w * slots + 1 + i) : 8 * (w * slots + i);
+        out[k++] = m;
+    }
+    *n = k;
     return OG_OK;
 }
 

@@ -11,10 +11,6 @@
 
 using namespace og;
 
-struct og_filters {
-    FilterSet set;
-};
-
 extern "C" {
 
 void og_secret_scalar(const uint8_t seed[32], uint8_t scalar[32]) { secret_scalar(seed, scalar); }

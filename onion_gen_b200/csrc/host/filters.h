@@ -82,3 +82,9 @@ std::vector<uint64_t> build_bitmap(const std::vector<PrefixFilter>& filters, uin
 double bitmap_occupancy(const std::vector<uint64_t>& words, uint32_t bits);
 
 }  // namespace og
+
+// The C ABI's filter-set handle (og_filters_new), shared with the engine's
+// device exact match.
+struct og_filters {
+    og::FilterSet set;
+};

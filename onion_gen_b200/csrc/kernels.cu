@@ -99,7 +99,30 @@ __global__ void __launch_bounds__(OG_LB_THREADS, 5) chain_kernel(const ChainArgs
     store_fe(a.lanes + 6 * L + lane, L, T);
 }
 
+// Exact match of one advance's bitmap survivors (grid-stride; the survivor
+// count is read on the device, so the launch needs no host round trip).
+__global__ void __launch_bounds__(256) match_kernel(const MatchArgs a) {
+    const uint32_t n = min(*a.surv_count, a.surv_cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const HitRec r = a.surv[i];
+        const uint32_t owner = exact_owner(a.t, r.y[0], r.y[1]);
+        if (owner != 0xffffffffu) {
+            const uint32_t idx = atomicAdd(a.out_count, 1u);
+            if (idx < a.out_cap) {
+                HitRec h = r;
+                h.pad = owner;
+                a.out[idx] = h;
+            }
+        }
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_match(const MatchArgs& a, int grid, cudaStream_t s) {
+    match_kernel<<<grid, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_init(const InitArgs& a, int block, cudaStream_t s) {
     const unsigned grid = (a.lanes_n + block - 1) / block;

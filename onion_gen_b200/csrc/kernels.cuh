@@ -89,7 +89,35 @@ struct InitArgs {
     uint32_t affine_out;
 };
 
+// Exact-match tables of a literal-prefix filter set in the form the device
+// searches (FilterSet::match_key, src/filter.rs:2194-2213, with the length
+// buckets of :2645-2700): one bucket per distinct filter length of at most
+// 12 symbols, each a sorted run of masked 64-bit key heads (bytes 0..7 of the
+// packed key, big-endian) with the owning filter's index.
+constexpr int MAX_MATCH_BUCKETS = 12;
+struct MatchTables {
+    const uint64_t* keys;
+    const uint32_t* owners;
+    uint32_t nbuckets;
+    uint32_t bucket_bits[MAX_MATCH_BUCKETS];
+    uint32_t bucket_off[MAX_MATCH_BUCKETS];
+    uint32_t bucket_len[MAX_MATCH_BUCKETS];
+};
+
+// The single engine's exact match over one advance's bitmap survivors:
+// matching records are copied to `out` with `pad` = the filter's index.
+struct MatchArgs {
+    const HitRec* surv;
+    const uint32_t* surv_count;
+    uint32_t surv_cap;
+    MatchTables t;
+    HitRec* out;
+    uint32_t* out_count;
+    uint32_t out_cap;
+};
+
 cudaError_t launch_init(const InitArgs& a, int block, cudaStream_t s);
+cudaError_t launch_match(const MatchArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_paired(const PairedArgs& a, int block, cudaStream_t s);
 cudaError_t launch_chain(const ChainArgs& a, int block, cudaStream_t s);
 

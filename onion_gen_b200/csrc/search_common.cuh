@@ -71,6 +71,26 @@ __device__ __forceinline__ void test_emit(const Sink& k, const fe& yraw, uint32_
     }
 }
 
+// The filter a canonical key matches exactly on its first 12 symbols at
+// most, or 0xffffffff: per length bucket, a binary search of the sorted
+// masked heads. No kept filter is a prefix of another, so at most one
+// matches.
+__device__ __forceinline__ uint32_t exact_owner(const MatchTables& t, const uint32_t y0, const uint32_t y1) {
+    const uint64_t head = ((uint64_t)__byte_perm(y0, 0, 0x0123) << 32) | (uint64_t)__byte_perm(y1, 0, 0x0123);
+    for (uint32_t b = 0; b < t.nbuckets; b++) {
+        const uint64_t probe = head & (~0ULL << (64 - t.bucket_bits[b]));
+        const uint64_t* k = t.keys + t.bucket_off[b];
+        uint32_t lo = 0, hi = t.bucket_len[b];
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (k[mid] < probe) lo = mid + 1;
+            else hi = mid;
+        }
+        if (lo < t.bucket_len[b] && k[lo] == probe) return t.owners[t.bucket_off[b] + lo];
+    }
+    return 0xffffffffu;
+}
+
 // p3 + cached addend with Z = 1: seven multiplications
 // (the formulas of src/curve.rs:130-175 with the addend's Z scaled away).
 __device__ __forceinline__ void add_cached(fe& X, fe& Y, fe& Z, fe& T, const fe& ypx, const fe& ymx,

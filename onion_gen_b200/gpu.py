@@ -134,3 +134,25 @@ class Engine:
     def advance(self):
         offsets, packed = self.advance_raw()
         return [Survivor(int(o), bytes(p)) for o, p in zip(offsets, packed)]
+
+    def match_on_device(self, filters):
+        """Exact match on the device from now on (og_engine_match_on_device):
+        ``filters`` is the ``filter.FilterSet`` whose index_words this engine
+        was created with."""
+        err = N.errbuf()
+        N.check(N.lib.og_engine_match_on_device(self._h, filters._h, err, 512), err)
+        self._mbuf = (N.Match * max(self._room, 1))()
+
+    def advance_matches_raw(self):
+        """One advance returning only exact matches, as numpy arrays:
+        (offsets uint64[n], packed uint8[n, 32], filter index uint32[n])."""
+        if getattr(self, "_mbuf", None) is None:
+            raise N.OgError(8, "match_on_device() has not been called")
+        n = C.c_size_t()
+        err = N.errbuf()
+        N.check(N.lib.og_engine_advance_matches(self._h, self._mbuf, self._room, C.byref(n), err, 512), err)
+        k = n.value
+        raw = np.frombuffer(self._mbuf, dtype=np.uint8, count=k * 48).reshape(k, 48)
+        offsets = raw[:, :8].copy().view(np.uint64).reshape(k)
+        filters = raw[:, 40:44].copy().view(np.uint32).reshape(k)
+        return offsets, raw[:, 8:40].copy(), filters

@@ -26,11 +26,17 @@ class Found:
     filter: int
 
 
-def device_search(device, seed: bytes, prefixes, quota: int, threads: int = 0, config=None, max_advances=None):
+def device_search(device, seed: bytes, prefixes, quota: int, threads: int = 0, config=None, max_advances=None,
+                  device_match=False):
+    """``device_match`` moves the exact match onto the device
+    (og_engine_advance_matches): only matches cross back, the same ones the
+    host match finds."""
     fs = F.FilterSet.parse_all(prefixes)
     words, bits = fs.index_words()
     start = key.start_point(seed)
     eng = gpu.Engine(device, start, threads=threads, bitmap=words, bitmap_bits=bits, config=config)
+    if device_match:
+        eng.match_on_device(fs)
     texts = fs.texts()
     found = []
     advances = 0
@@ -39,11 +45,15 @@ def device_search(device, seed: bytes, prefixes, quota: int, threads: int = 0, c
         while len(found) < quota:
             if max_advances is not None and advances >= max_advances:
                 break
-            offsets, packed = eng.advance_raw()
+            if device_match:
+                offsets, packed, matched = eng.advance_matches_raw()
+                idx = np.arange(len(offsets))
+            else:
+                offsets, packed = eng.advance_raw()
+                matched = fs.match_many(packed)  # the bitmap says maybe, the exact check decides
+                idx = np.nonzero(matched >= 0)[0]
             advances += 1
             examined += eng.batch()
-            matched = fs.match_many(packed)  # the bitmap says maybe, the exact check decides
-            idx = np.nonzero(matched >= 0)[0]
             # this advance's range lies above every earlier one: its matches
             # in offset order are the next hits, up to the quota
             for j in idx[np.argsort(offsets[idx], kind="stable")]:

@@ -1,0 +1,115 @@
+"""Device-side exact match of the single engine (og_engine_match_on_device,
+og_engine_advance_matches) against the host's FilterSet::match_key over the
+same engine's survivors (runs on a B200: -m gpu).
+
+Two engines of one shape from one start: the first returns its bitmap
+survivors and the host matches them (run::device_worker, src/run.rs:1081-1085);
+the second matches on the device. The two match lists must be equal —
+offsets, keys and filter indices — including filters longer than the 12
+symbols the device tables hold, which the host confirms.
+"""
+import numpy as np
+import pytest
+
+from onion_gen_b200 import _native as N
+from onion_gen_b200 import filter as F
+from onion_gen_b200 import gpu, key, workloads
+
+pytestmark = pytest.mark.gpu
+
+HALF, LANES, ROUNDS = 128, 1024, 8
+SLOTS = 2 * HALF + 1
+
+
+def cfg(dump=0):
+    return N.EngineConfig(N.SCHEME_PAIRED, HALF, LANES, ROUNDS, 128, dump, 0)
+
+
+def key_at(seed, offset):
+    secret = key.expanded_secret_at_offset(seed, offset)
+    return key.pack(key.scalar_base_mult(secret[:32]))
+
+
+def host_matches(eng, fs, advances):
+    out = []
+    for _ in range(advances):
+        o, k = eng.advance_raw()
+        m = fs.match_many(k)
+        for j in np.nonzero(m >= 0)[0]:
+            out.append((int(o[j]), bytes(k[j]), int(m[j])))
+    return sorted(out)
+
+
+def device_matches(eng, advances):
+    out = []
+    for _ in range(advances):
+        o, k, f = eng.advance_matches_raw()
+        out.extend((int(a), bytes(b), int(c)) for a, b, c in zip(o, k, f))
+    return sorted(out)
+
+
+def test_device_match_equals_host_match(device):
+    seed = workloads.seed(0)
+    start = key.start_point(seed)
+    # config 3's prefixes plus long filters built from a key the first
+    # advance examines: one that matches it on 14 symbols, one that shares
+    # its first 12 symbols and differs after (the device cannot tell them
+    # apart), and one of 20 symbols that matches
+    off = 8 * (5 * SLOTS + 1 + 17)
+    text = key.address(key_at(seed, off))
+    decoy = text[:12] + ("a" if text[12] != "a" else "b") + text[13]
+    prefixes = workloads.config3_prefixes(2000) + [text[:14], decoy, text[:20]]
+    fs = F.FilterSet.parse_all(prefixes)
+    words, bits = fs.index_words()
+    plain = gpu.Engine(device, start, bitmap=words, bitmap_bits=bits, config=cfg())
+    want = host_matches(plain, fs, 2)
+    plain.close()
+    matched = gpu.Engine(device, start, bitmap=words, bitmap_bits=bits, config=cfg())
+    matched.match_on_device(fs)
+    got = device_matches(matched, 2)
+    matched.close()
+    assert len(want) > 1000
+    assert got == want
+    # the constructed key is found, owned by its 14-symbol filter (the
+    # 20-symbol one is absorbed by it)
+    texts = fs.texts()
+    hit = [g for g in got if g[0] == off]
+    assert len(hit) == 1 and texts[hit[0][2]] == text[:14]
+    assert decoy in texts
+    for o, packed, f in got[:100]:
+        pk, _ = key.check_hit(seed, o, packed)
+        assert key.address(pk).startswith(texts[f])
+
+
+def test_device_match_refuses_a_different_filter_set(device):
+    start = key.start_point(workloads.seed(0))
+    fs = F.FilterSet.parse_all(["abc"])
+    other = F.FilterSet.parse_all(["abd"])
+    words, bits = fs.index_words()
+    eng = gpu.Engine(device, start, bitmap=words, bitmap_bits=bits, config=cfg())
+    with pytest.raises(N.OgError) as e:
+        eng.advance_matches_raw()
+    assert e.value.status == "OG_E_STATE"
+    with pytest.raises(N.OgError) as e:
+        eng.match_on_device(other)
+    assert e.value.status == "OG_E_ARG"
+    eng.match_on_device(fs)
+    o, k, f = eng.advance_matches_raw()
+    assert all(fs.match_key(bytes(p)) == 0 for p in k)
+    dump = gpu.Engine(device, start, config=cfg(dump=1))
+    with pytest.raises(N.OgError) as e:
+        dump.match_on_device(fs)
+    assert e.value.status == "OG_E_STATE"
+
+
+def test_run_driver_finds_the_same_hits_with_the_device_match(device):
+    from onion_gen_b200 import run
+
+    searches = [s for s in workloads.config4_searches() if s.quota / sum(32.0 ** -len(p) for p in s.prefixes) < 2e7]
+    assert len(searches) >= 2
+    for s in searches[:3]:
+        host, ex_h, adv_h = run.device_search(device, s.seed, s.prefixes, s.quota, config=cfg(), max_advances=40)
+        dev, ex_d, adv_d = run.device_search(device, s.seed, s.prefixes, s.quota, config=cfg(), max_advances=40,
+                                             device_match=True)
+        assert len(host) == s.quota
+        assert dev == host and (ex_d, adv_d) == (ex_h, adv_h)

@@ -132,14 +132,26 @@ typedef struct og_match {
 
 /* Turns the device match on. `f` must be the filter set whose index_words the
  * engine was created with (same width and the same bitmap, checked:
- * OG_E_ARG otherwise); its exact-match tables are copied and `f` is not
+ * OG_E_ARG otherwise) and hold no suffix (an engine from og_engine_new has
+ * no suffix bitmap); its exact-match tables are copied and `f` is not
  * referenced afterwards. An engine created with dump = 1 has no bitmap and
  * refuses (OG_E_STATE). */
 int og_engine_match_on_device(og_engine* e, const struct og_filters* f, char* err, size_t errlen);
 
+/* An engine over a whole filter set, prefixes and suffixes (shape as
+ * og_engine_new_config; dump must be 0), with the device match already on.
+ * Candidates survive the kernel through the prefix bitmap or the suffix
+ * bitmap (og_filters_suffix_words); a suffix survivor's key is recomputed
+ * on the device from its offset, sign bit and SHA3-256 checksum included
+ * (src/key.rs:106-132), and matched on its address. Suffix matches carry
+ * filter index og_filters_prefix_count(f) + j. */
+int og_engine_new_filters(int ordinal, const uint8_t start[128], const struct og_filters* f,
+                          const og_engine_config* cfg, og_engine** out, char* err, size_t errlen);
+
 /* One advance that returns only the exact matches (room `cap`, count `*n`).
  * Survivors beyond the engine's room are OG_E_OVERFLOW as in
- * og_engine_advance. Filters longer than 12 symbols are matched on their
+ * og_engine_advance; a recomputed suffix key that differs from the search
+ * kernel's is OG_E_VERIFY. Filters longer than 12 symbols are matched on their
  * first 12 on the device and confirmed on the host before they are
  * returned. */
 int og_engine_advance_matches(og_engine* e, og_match* out, size_t cap, size_t* n, char* err, size_t errlen);
@@ -349,17 +361,36 @@ void og_block_seed(const uint8_t root[32], uint64_t index, uint8_t out[32]);
 int og_check_hit(const uint8_t seed[32], uint64_t offset, const uint8_t packed[32], uint8_t pk[32],
                  uint8_t secret[64]);
 
-/* ---- prefix filters: FilterSet (src/filter.rs) ------------------------- */
+/* ---- filters: FilterSet (src/filter.rs) -------------------------------- */
 
 typedef struct og_filters og_filters;
 
-/* Newline-separated literal prefixes; bits = 0 chooses the index width. */
+/* Newline-separated filters (Pattern::parse, src/filter.rs:298-350): literal
+ * prefixes (bare, `^` or `prefix:`) and `suffix:` forms whose symbols may
+ * be `?` or `[...]` classes (parse_symbols, :495-560), checked against the
+ * v3 address tail (:566-600). `bits` is the prefix index width, 0 to choose
+ * it; the suffix index width is always chosen (:1420-1440). A suffix that
+ * reaches too little of the key for a suffix bitmap is OG_E_FILTER. */
 int og_filters_new(const char* text, uint32_t bits, og_filters** out, char* err, size_t errlen);
+/* Kept filters: the prefixes (sorted, absorbed) first, then the suffixes
+ * (sorted, duplicates dropped). */
 size_t og_filters_count(const og_filters* f);
-/* canonical text of kept filter i (sorted, absorbed) */
+size_t og_filters_prefix_count(const og_filters* f);
+/* canonical text of kept filter i ("suffix:..." for a suffix) */
 int og_filters_text(const og_filters* f, size_t i, char* out, size_t cap);
+/* The prefix index (FilterSet::index_words, src/filter.rs:1857); 0 words
+ * when the set has no prefix. */
 uint32_t og_filters_bits(const og_filters* f);
 size_t og_filters_words(const og_filters* f, const uint64_t** words);
+/* The suffix index (BitmapIndex::build_over_suffixes, src/filter.rs:2406):
+ * keyed on base32 bits [255 - bits, 255) of the packed key; 0 words when the
+ * set has no suffix. */
+uint32_t og_filters_suffix_bits(const og_filters* f);
+size_t og_filters_suffix_words(const og_filters* f, const uint64_t** words);
+/* The full check of a public key (sign bit included) against every filter,
+ * on its address (FilterSet::match_address, src/filter.rs:2152): the index
+ * of the first match or -1. */
+long og_filters_match_address(const og_filters* f, const uint8_t pk[32]);
 double og_filters_occupancy(const og_filters* f);
 /* FilterSet::match_key (src/filter.rs:2098): index of the match or -1. */
 long og_filters_match(const og_filters* f, const uint8_t packed[32]);

@@ -150,6 +150,7 @@ def _load():
     sig("og_engine_advance", I, [P, P, SZ, C.POINTER(SZ), B, SZ])
     sig("og_engine_last_kernel_ms", C.c_float, [P])
     sig("og_engine_match_on_device", I, [P, P, B, SZ])
+    sig("og_engine_new_filters", I, [I, B, P, P, C.POINTER(P), B, SZ])
     sig("og_engine_advance_matches", I, [P, P, SZ, C.POINTER(SZ), B, SZ])
     sig("og_engine_free", None, [P])
     sig("og_batch_new", I, [I, C.POINTER(BatchConfig), C.POINTER(P), B, SZ])
@@ -190,6 +191,10 @@ def _load():
     sig("og_filters_occupancy", C.c_double, [P])
     sig("og_filters_match", C.c_long, [P, B])
     sig("og_filters_match_many", SZ, [P, P, SZ, SZ, P])
+    sig("og_filters_prefix_count", SZ, [P])
+    sig("og_filters_suffix_bits", U32, [P])
+    sig("og_filters_suffix_words", SZ, [P, C.POINTER(C.POINTER(U64))])
+    sig("og_filters_match_address", C.c_long, [P, B])
     sig("og_filters_free", None, [P])
     return L
 

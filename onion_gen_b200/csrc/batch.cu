@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(OG_LB_THREADS, OG_LB_MIN_BLOCKS) batch_search_
         if (sb.sidx == NONE) continue;
         const BatchDesc& d = a.descs[sb.sidx];
         const uint32_t slot = item * BLOCK + threadIdx.x;
-        const Sink sink{d.bitmap, d.bits, a.surv, &a.counters->surv, a.surv_cap, sb.sidx};
+        const Sink sink{d.bitmap, d.bits, a.surv, &a.counters->surv, a.surv_cap, sb.sidx, nullptr, 0};
         fe x = load_fe(a.lanes + 0 * a.slots + slot, a.slots);
         fe y = load_fe(a.lanes + 2 * a.slots + slot, a.slots);
         paired_rounds(x, y, words_fe(d.wx), words_fe(d.wy), words_fe(d.wt), qtab, a.half, a.rounds,

@@ -151,15 +151,22 @@ struct og_engine {
     PairedArgs pa{};
     ChainArgs ca{};
     uint64_t bitmap_hash = 0;  // of the bitmap the engine was created with
+    DevBuf<uint32_t> sbitmap;  // suffix bitmap (og_engine_new_filters)
+    uint32_t sbits = 0;
+    Pt start{};
     // device exact match (og_engine_match_on_device)
     bool matching = false;
     bool long_filters = false;  // some filter is longer than the device tables reach
+    uint32_t prefix_count = 0;
     og::FilterSet fs;
     DevBuf<uint64_t> mkeys;
     DevBuf<uint32_t> mowners, mcount;
     DevBuf<HitRec> matches;
     HostBuf<HitRec> h_matches;
     HostBuf<uint32_t> h_mcount;
+    DevBuf<uint32_t> suffixes, mismatch;
+    HostBuf<uint32_t> h_mismatch;
+    DevBuf<uint4> pow8;
     MatchArgs ma{};
 
     ~og_engine() {
@@ -205,16 +212,25 @@ size_t room_for(uint64_t batch, bool dump, double occupancy) {
     return (size_t)std::min<double>((double)batch, std::max(4096.0, want));
 }
 
+// `f` (may be null) supplies both bitmaps instead of `bitmap`: its prefix
+// index (if it has prefixes) and its suffix index (if it has suffixes).
 int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, const uint64_t* bitmap, size_t words,
-                 uint32_t bits, og_engine** out, char* err, size_t errlen) {
+                 uint32_t bits, og_engine** out, char* err, size_t errlen, const og_filters* f = nullptr) {
     if (!out || !start) return fail(err, errlen, OG_E_ARG, "null argument");
     *out = nullptr;
+    const bool suffixed = f && f->has_suffixes;
+    if (f) {
+        if (cfg.dump) return fail(err, errlen, OG_E_ARG, "a filter engine cannot keep every candidate (dump)");
+        bitmap = f->has_prefixes ? f->set.words().data() : nullptr;
+        words = f->has_prefixes ? f->set.words().size() : 0;
+        bits = f->has_prefixes ? f->set.bits() : 0;
+    }
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
         return fail(err, errlen, OG_E_NODEVICE, "no CUDA device is available");
     if (ordinal < 0 || ordinal >= count) return fail(err, errlen, OG_E_ARG, "device %d of %d", ordinal, count);
     if (cfg.scheme > OG_SCHEME_CHAIN) return fail(err, errlen, OG_E_ARG, "unknown scheme %u", cfg.scheme);
-    if (!cfg.dump) {
+    if (!cfg.dump && (bitmap || !suffixed)) {
         if (!bitmap) return fail(err, errlen, OG_E_ARG, "no bitmap: without one every candidate would cross back");
         if (bits < 8 || bits > 32) return fail(err, errlen, OG_E_ARG, "bitmap width %u outside 8..32", bits);
         const size_t need = (size_t)(((1ULL << bits) + 63) / 64);
@@ -243,8 +259,12 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
     }
     double occupancy = 1.0;
     if (!cfg.dump) {
-        std::vector<uint64_t> w(bitmap, bitmap + (size_t)(((1ULL << bits) + 63) / 64));
-        occupancy = bitmap_occupancy(w, bits);
+        occupancy = 0.0;
+        if (bitmap) {
+            std::vector<uint64_t> w(bitmap, bitmap + (size_t)(((1ULL << bits) + 63) / 64));
+            occupancy = bitmap_occupancy(w, bits);
+        }
+        if (suffixed) occupancy += f->suffixes.occupancy();
         // keep the survivor buffer of one advance within 2^24 records
         while (cfg.rounds > 1 && 4.0 * (double)cfg.lanes * slots * cfg.rounds * occupancy > (double)(1u << 24))
             cfg.rounds /= 2;
@@ -276,12 +296,20 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
     CU(e->hits.alloc(e->cap));
     CU(e->h_hits.alloc(e->cap));
     CU(e->h_counter.alloc(1));
-    if (!cfg.dump) {
+    if (!cfg.dump && bitmap) {
         const size_t w32 = (size_t)(((1ULL << bits) + 31) / 32);
         CU(e->bitmap.alloc(std::max<size_t>(w32, 2)));
         CU(cudaMemcpyAsync(e->bitmap.p, bitmap, w32 * 4, cudaMemcpyHostToDevice, e->stream));
         e->bitmap_hash = words_hash(bitmap, (size_t)(((1ULL << bits) + 63) / 64));
     }
+    if (suffixed) {
+        const uint32_t sb = f->suffixes.bits();
+        const size_t w32 = (size_t)(((1ULL << sb) + 31) / 32);
+        CU(e->sbitmap.alloc(std::max<size_t>(w32, 2)));
+        CU(cudaMemcpyAsync(e->sbitmap.p, f->suffixes.words().data(), w32 * 4, cudaMemcpyHostToDevice, e->stream));
+        e->sbits = sb;
+    }
+    e->start = start_pt;
 
     // lane start points
     InitArgs ia{};
@@ -321,6 +349,8 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
         a.scratch = e->scratch.p;
         a.bitmap = cfg.dump ? nullptr : e->bitmap.p;
         a.bits = bits;
+        a.sbitmap = e->sbitmap.p;
+        a.sbits = e->sbits;
         a.hits = e->hits.p;
         a.counter = e->counter.p;
         a.cap = (uint32_t)std::min<size_t>(e->cap, 0xffffffffu);
@@ -338,6 +368,8 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
         a.scratch = e->scratch.p;
         a.bitmap = cfg.dump ? nullptr : e->bitmap.p;
         a.bits = bits;
+        a.sbitmap = e->sbitmap.p;
+        a.sbits = e->sbits;
         a.hits = e->hits.p;
         a.counter = e->counter.p;
         a.cap = (uint32_t)std::min<size_t>(e->cap, 0xffffffffu);
@@ -368,6 +400,83 @@ double time_advance(og_engine* e, std::vector<og_survivor>& buf) {
     if (og_engine_advance(e, buf.data(), buf.size(), &n, nullptr, 0) != OG_OK) return -1;
     const double ms = e->last_ms;
     return ms > 0 ? (double)og_engine_batch(e) / (ms * 1e-3) : -1;
+}
+
+
+// Device exact match for `f`: prefix tables, suffix patterns, the table of
+// 2^j 8G the suffix confirmation walks, and the match buffers.
+int enable_matching(og_engine* e, const og_filters* f, char* err, size_t errlen) {
+    std::vector<FilterSet::DeviceBucket> buckets;
+    std::vector<uint64_t> keys;
+    std::vector<uint32_t> owners;
+    if (f->has_prefixes) f->set.device_tables(buckets, keys, owners);
+    if (buckets.size() > (size_t)MAX_MATCH_BUCKETS)
+        return fail(err, errlen, OG_E_FILTER, "more than %d filter lengths", MAX_MATCH_BUCKETS);
+    std::vector<uint32_t> sfx;
+    if (f->has_suffixes) {
+        for (size_t j = 0; j < f->suffixes.size(); j++) {
+            const SuffixPattern& p = f->suffixes.pattern(j);
+            std::vector<uint32_t> row(MAX_SUFFIX_SYMBOLS + 1, 0);
+            row[0] = (uint32_t)p.sets.size();
+            for (size_t i = 0; i < p.sets.size(); i++) row[1 + i] = p.sets[i];
+            sfx.insert(sfx.end(), row.begin(), row.end());
+        }
+    }
+    e->matching = false;
+    CU(cudaSetDevice(e->device));
+    CU(cudaStreamSynchronize(e->stream));
+    CU(e->mkeys.alloc(std::max<size_t>(keys.size(), 1)));
+    CU(e->mowners.alloc(std::max<size_t>(owners.size(), 1)));
+    if (!keys.empty()) {
+        CU(cudaMemcpyAsync(e->mkeys.p, keys.data(), keys.size() * 8, cudaMemcpyHostToDevice, e->stream));
+        CU(cudaMemcpyAsync(e->mowners.p, owners.data(), owners.size() * 4, cudaMemcpyHostToDevice, e->stream));
+    }
+    std::vector<uint4> pw;
+    if (!sfx.empty()) {
+        CU(e->suffixes.alloc(sfx.size()));
+        CU(cudaMemcpyAsync(e->suffixes.p, sfx.data(), sfx.size() * 4, cudaMemcpyHostToDevice, e->stream));
+        pw = pow2_table(base_mult_u64(8), 64);
+        CU(e->pow8.alloc(pw.size()));
+        CU(cudaMemcpyAsync(e->pow8.p, pw.data(), pw.size() * sizeof(uint4), cudaMemcpyHostToDevice, e->stream));
+    }
+    CU(e->mcount.alloc(1));
+    CU(e->h_mcount.alloc(1));
+    CU(e->mismatch.alloc(1));
+    CU(e->h_mismatch.alloc(1));
+    CU(e->matches.alloc(e->cap));
+    CU(e->h_matches.alloc(e->cap));
+    CU(cudaStreamSynchronize(e->stream));
+    e->fs = f->set;
+    e->long_filters = false;
+    if (f->has_prefixes)
+        for (size_t i = 0; i < e->fs.size(); i++)
+            if (e->fs.filter(i).text.size() > FilterSet::DEVICE_SYMBOLS) e->long_filters = true;
+    e->prefix_count = f->has_prefixes ? (uint32_t)f->set.size() : 0;
+    MatchArgs& m = e->ma;
+    m = MatchArgs{};
+    m.surv = e->hits.p;
+    m.surv_count = e->counter.p;
+    m.surv_cap = (uint32_t)std::min<size_t>(e->cap, 0xffffffffu);
+    m.t = match_tables(buckets, e->mkeys.p, e->mowners.p);
+    m.sbitmap = sfx.empty() ? nullptr : e->sbitmap.p;
+    m.sbits = e->sbits;
+    m.suffixes = e->suffixes.p;
+    m.nsuffix = f->has_suffixes ? (uint32_t)f->suffixes.size() : 0;
+    m.prefix_count = e->prefix_count;
+    m.sx = to_words(e->start.X);
+    m.sy = to_words(e->start.Y);
+    m.sz = to_words(e->start.Z);
+    m.st = to_words(e->start.T);
+    m.pow8 = e->pow8.p;
+    m.lanes = e->cfg.lanes;
+    m.slots = e->slots;
+    m.paired = e->cfg.scheme == OG_SCHEME_PAIRED ? 1u : 0u;
+    m.out = e->matches.p;
+    m.out_count = e->mcount.p;
+    m.out_cap = m.surv_cap;
+    m.mismatch = e->mismatch.p;
+    e->matching = true;
+    return OG_OK;
 }
 
 }  // namespace
@@ -401,6 +510,23 @@ int og_engine_new_config(int ordinal, const uint8_t start[128], const og_engine_
     og_engine_config c{};
     if (cfg) c = *cfg;
     return build_engine(ordinal, start, c, bitmap, words, bits, out, err, errlen);
+}
+
+int og_engine_new_filters(int ordinal, const uint8_t start[128], const og_filters* f, const og_engine_config* cfg,
+                          og_engine** out, char* err, size_t errlen) {
+    if (!f || !out) return fail(err, errlen, OG_E_ARG, "null argument");
+    og_engine_config c{};
+    if (cfg) c = *cfg;
+    og_engine* e = nullptr;
+    int rc = build_engine(ordinal, start, c, nullptr, 0, 0, &e, err, errlen, f);
+    if (rc != OG_OK) return rc;
+    rc = enable_matching(e, f, err, errlen);
+    if (rc != OG_OK) {
+        og_engine_free(e);
+        return rc;
+    }
+    *out = e;
+    return OG_OK;
 }
 
 int og_engine_new(int ordinal, const uint8_t start[128], uint32_t threads, const uint64_t* bitmap, size_t words,
@@ -533,46 +659,16 @@ int og_engine_advance(og_engine* e, og_survivor* out, size_t cap, size_t* n, cha
 int og_engine_match_on_device(og_engine* e, const og_filters* f, char* err, size_t errlen) {
     if (!e || !f) return fail(err, errlen, OG_E_ARG, "null argument");
     if (e->cfg.dump) return fail(err, errlen, OG_E_STATE, "the engine keeps every candidate: it has no bitmap to match behind");
-    if (f->set.bits() != e->bits)
-        return fail(err, errlen, OG_E_ARG, "the filter set's index is %u bits wide and the engine's %u", f->set.bits(),
-                    e->bits);
+    if (f->has_suffixes && !e->sbitmap.p)
+        return fail(err, errlen, OG_E_ARG,
+                    "the filter set has suffixes and the engine no suffix bitmap: create it with og_engine_new_filters");
+    if (!f->has_prefixes || f->set.bits() != e->bits)
+        return fail(err, errlen, OG_E_ARG, "the filter set's index is %u bits wide and the engine's %u",
+                    f->has_prefixes ? f->set.bits() : 0, e->bits);
     const size_t nwords = (size_t)(((1ULL << e->bits) + 63) / 64);
     if (f->set.words().size() < nwords || words_hash(f->set.words().data(), nwords) != e->bitmap_hash)
         return fail(err, errlen, OG_E_ARG, "the filter set's bitmap is not the one the engine was created with");
-    std::vector<FilterSet::DeviceBucket> buckets;
-    std::vector<uint64_t> keys;
-    std::vector<uint32_t> owners;
-    f->set.device_tables(buckets, keys, owners);
-    if (buckets.size() > (size_t)MAX_MATCH_BUCKETS)
-        return fail(err, errlen, OG_E_FILTER, "more than %d filter lengths", MAX_MATCH_BUCKETS);
-    e->matching = false;
-    CU(cudaSetDevice(e->device));
-    CU(cudaStreamSynchronize(e->stream));
-    CU(e->mkeys.alloc(std::max<size_t>(keys.size(), 1)));
-    CU(e->mowners.alloc(std::max<size_t>(owners.size(), 1)));
-    if (!keys.empty()) {
-        CU(cudaMemcpyAsync(e->mkeys.p, keys.data(), keys.size() * 8, cudaMemcpyHostToDevice, e->stream));
-        CU(cudaMemcpyAsync(e->mowners.p, owners.data(), owners.size() * 4, cudaMemcpyHostToDevice, e->stream));
-    }
-    CU(e->mcount.alloc(1));
-    CU(e->h_mcount.alloc(1));
-    CU(e->matches.alloc(e->cap));
-    CU(e->h_matches.alloc(e->cap));
-    CU(cudaStreamSynchronize(e->stream));
-    e->fs = f->set;
-    e->long_filters = false;
-    for (size_t i = 0; i < e->fs.size(); i++)
-        if (e->fs.filter(i).text.size() > FilterSet::DEVICE_SYMBOLS) e->long_filters = true;
-    MatchArgs& m = e->ma;
-    m.surv = e->hits.p;
-    m.surv_count = e->counter.p;
-    m.surv_cap = (uint32_t)std::min<size_t>(e->cap, 0xffffffffu);
-    m.t = match_tables(buckets, e->mkeys.p, e->mowners.p);
-    m.out = e->matches.p;
-    m.out_count = e->mcount.p;
-    m.out_cap = m.surv_cap;
-    e->matching = true;
-    return OG_OK;
+    return enable_matching(e, f, err, errlen);
 }
 
 int og_engine_advance_matches(og_engine* e, og_match* out, size_t cap, size_t* n, char* err, size_t errlen) {
@@ -583,6 +679,8 @@ int og_engine_advance_matches(og_engine* e, og_match* out, size_t cap, size_t* n
     CU(cudaSetDevice(e->device));
     CU(cudaMemsetAsync(e->counter.p, 0, sizeof(uint32_t), e->stream));
     CU(cudaMemsetAsync(e->mcount.p, 0, sizeof(uint32_t), e->stream));
+    CU(cudaMemsetAsync(e->mismatch.p, 0, sizeof(uint32_t), e->stream));
+    e->ma.window0 = e->launches * (uint64_t)e->cfg.rounds * e->cfg.lanes;
     CU(cudaEventRecord(e->ev0, e->stream));
     if (e->cfg.scheme == OG_SCHEME_PAIRED) {
         CU(launch_paired(e->pa, (int)e->cfg.block, e->stream));
@@ -595,6 +693,7 @@ int og_engine_advance_matches(og_engine* e, og_match* out, size_t cap, size_t* n
     CU(launch_match(e->ma, std::max(sms, 1) * 4, e->stream));
     CU(cudaMemcpyAsync(e->h_counter.p, e->counter.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream));
     CU(cudaMemcpyAsync(e->h_mcount.p, e->mcount.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream));
+    CU(cudaMemcpyAsync(e->h_mismatch.p, e->mismatch.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream));
     CU(cudaStreamSynchronize(e->stream));
     cudaEventElapsedTime(&e->last_ms, e->ev0, e->ev1);
     const uint64_t launch = e->launches++;
@@ -606,6 +705,10 @@ int og_engine_advance_matches(og_engine* e, og_match* out, size_t cap, size_t* n
                     "is filtering: a wider index is the answer",
                     found, e->cap);
     }
+    if (*e->h_mismatch.p)
+        return fail(err, errlen, OG_E_VERIFY,
+                    "%u survivors' keys recomputed from their offsets differ from the search kernel's",
+                    *e->h_mismatch.p);
     const uint32_t matched = *e->h_mcount.p;  // at most `found`, so within the buffer
     if (matched) {
         CU(cudaMemcpyAsync(e->h_matches.p, e->matches.p, (size_t)matched * sizeof(HitRec), cudaMemcpyDeviceToHost,
@@ -625,7 +728,7 @@ int og_engine_advance_matches(og_engine* e, og_match* out, size_t cap, size_t* n
         // With filters longer than the device tables reach, several can share
         // the 12 symbols the device compared: the host's match decides which
         // (if any) matches.
-        if (e->long_filters) {
+        if (e->long_filters && h.pad < e->prefix_count) {
             const long f = e->fs.match_key(m.packed);
             if (f < 0) continue;
             m.filter = (uint32_t)f;

@@ -50,49 +50,102 @@ int og_filters_new(const char* text, uint32_t bits, og_filters** out, char* err,
     if (!text || !out) return fail(err, errlen, OG_E_ARG, "null argument");
     *out = nullptr;
     std::vector<PrefixFilter> fs;
+    std::vector<SuffixPattern> sfx;
     const char* p = text;
     size_t line = 0;
     while (*p) {
         const char* e = std::strchr(p, '\n');
         std::string s = e ? std::string(p, (size_t)(e - p)) : std::string(p);
         line++;
-        bool blank = true;
-        for (char c : s)
-            if (c != ' ' && c != '\t' && c != '\r') blank = false;
-        if (!blank) {
-            PrefixFilter f;
+        size_t a = 0;
+        while (a < s.size() && (s[a] == ' ' || s[a] == '\t' || s[a] == '\r')) a++;
+        if (a < s.size()) {
             std::string why;
-            if (!parse_prefix(s, f, why)) return fail(err, errlen, OG_E_FILTER, "line %zu: %s", line, why.c_str());
-            fs.push_back(f);
+            const size_t colon = s.find(':');
+            std::string form = colon == std::string::npos ? "" : s.substr(a, colon - a);
+            while (!form.empty() && (form.back() == ' ' || form.back() == '\t')) form.pop_back();
+            for (char& c : form) c = (char)std::tolower((unsigned char)c);
+            if (form == "suffix") {
+                SuffixPattern sp;
+                if (!parse_suffix(s.substr(colon + 1), sp, why))
+                    return fail(err, errlen, OG_E_FILTER, "line %zu: %s", line, why.c_str());
+                sfx.push_back(sp);
+            } else {
+                PrefixFilter f;
+                if (!parse_prefix(s, f, why)) return fail(err, errlen, OG_E_FILTER, "line %zu: %s", line, why.c_str());
+                fs.push_back(f);
+            }
         }
         if (!e) break;
         p = e + 1;
     }
+    if (fs.empty() && sfx.empty()) return fail(err, errlen, OG_E_FILTER, "no filters");
     og_filters* h = new (std::nothrow) og_filters();
     if (!h) return fail(err, errlen, OG_E_NOMEM, "host memory");
     std::string why;
-    if (!h->set.build(std::move(fs), bits, why)) {
-        delete h;
-        return fail(err, errlen, OG_E_FILTER, "%s", why.c_str());
+    if (!fs.empty()) {
+        if (!h->set.build(std::move(fs), bits, why)) {
+            delete h;
+            return fail(err, errlen, OG_E_FILTER, "%s", why.c_str());
+        }
+        h->has_prefixes = true;
+    }
+    if (!sfx.empty()) {
+        if (!h->suffixes.build(std::move(sfx), 0, why)) {
+            delete h;
+            return fail(err, errlen, OG_E_FILTER, "%s", why.c_str());
+        }
+        h->has_suffixes = true;
     }
     *out = h;
     return OG_OK;
 }
 
-size_t og_filters_count(const og_filters* f) { return f ? f->set.size() : 0; }
+size_t og_filters_count(const og_filters* f) {
+    return f ? (f->has_prefixes ? f->set.size() : 0) + (f->has_suffixes ? f->suffixes.size() : 0) : 0;
+}
+
+size_t og_filters_prefix_count(const og_filters* f) { return f && f->has_prefixes ? f->set.size() : 0; }
 
 int og_filters_text(const og_filters* f, size_t i, char* out, size_t cap) {
-    if (!f || i >= f->set.size() || !out || cap == 0) return OG_E_ARG;
-    snprintf(out, cap, "%s", f->set.filter(i).text.c_str());
+    if (!f || i >= og_filters_count(f) || !out || cap == 0) return OG_E_ARG;
+    const size_t np = og_filters_prefix_count(f);
+    snprintf(out, cap, "%s", i < np ? f->set.filter(i).text.c_str() : f->suffixes.pattern(i - np).text.c_str());
     return OG_OK;
 }
 
-uint32_t og_filters_bits(const og_filters* f) { return f ? f->set.bits() : 0; }
+uint32_t og_filters_bits(const og_filters* f) { return f && f->has_prefixes ? f->set.bits() : 0; }
 
 size_t og_filters_words(const og_filters* f, const uint64_t** words) {
-    if (!f) return 0;
+    if (!f || !f->has_prefixes) return 0;
     if (words) *words = f->set.words().data();
     return f->set.words().size();
+}
+
+uint32_t og_filters_suffix_bits(const og_filters* f) { return f && f->has_suffixes ? f->suffixes.bits() : 0; }
+
+size_t og_filters_suffix_words(const og_filters* f, const uint64_t** words) {
+    if (!f || !f->has_suffixes) return 0;
+    if (words) *words = f->suffixes.words().data();
+    return f->suffixes.words().size();
+}
+
+long og_filters_match_address(const og_filters* f, const uint8_t pk[32]) {
+    if (!f || !pk) return -1;
+    if (f->has_prefixes) {
+        const long m = f->set.match_key(pk);
+        if (m >= 0) {
+            const PrefixFilter& pf = f->set.filter((size_t)m);
+            if (!pf.needs_full_check() || address(pk).compare(0, pf.text.size(), pf.text) == 0) return m;
+        }
+    }
+    if (f->has_suffixes) {
+        uint8_t addr[35];
+        address_bytes(pk, addr);
+        const long j = f->suffixes.match_address(addr);
+        if (j >= 0) return (long)og_filters_prefix_count(f) + j;
+    }
+    return -1;
 }
 
 double og_filters_occupancy(const og_filters* f) { return f ? f->set.occupancy() : 0.0; }

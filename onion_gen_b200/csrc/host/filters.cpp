@@ -195,9 +195,10 @@ bool FilterSet::build(std::vector<PrefixFilter> filters, uint32_t bits, std::str
     return true;
 }
 
-double FilterSet::occupancy() const { return bitmap_occupancy(words_, bits_); }
+double FilterSet::occupancy() const { return words_.empty() ? 0.0 : bitmap_occupancy(words_, bits_); }
 
 bool FilterSet::may_match(const uint8_t packed[32]) const {
+    if (words_.empty()) return false;  // a set with no prefixes
     const size_t s = slot_of(packed, bits_);
     return (words_[s >> 6] >> (s & 63)) & 1;
 }

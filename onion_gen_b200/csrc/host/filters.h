@@ -14,6 +14,8 @@
 #include <string>
 #include <vector>
 
+#include "suffix.h"
+
 namespace og {
 
 constexpr size_t KEY_ONLY_SYMBOLS = 49;
@@ -84,7 +86,11 @@ double bitmap_occupancy(const std::vector<uint64_t>& words, uint32_t bits);
 }  // namespace og
 
 // The C ABI's filter-set handle (og_filters_new), shared with the engine's
-// device exact match.
+// device exact match: the literal prefixes and the suffixes of one set.
+// Filter index i < set.size() is prefix i; set.size() + j is suffix j.
 struct og_filters {
     og::FilterSet set;
+    og::SuffixSet suffixes;
+    bool has_prefixes = false;
+    bool has_suffixes = false;
 };

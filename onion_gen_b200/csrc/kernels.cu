@@ -2,6 +2,7 @@
 // candidate numbering; field.cuh for the arithmetic.
 #include "field.cuh"
 #include "kernels.cuh"
+#include "keccak.cuh"
 #include "search_common.cuh"
 
 // Register budget of the search kernels: at most OG_LB_THREADS threads per
@@ -52,7 +53,7 @@ __global__ void __launch_bounds__(OG_LB_THREADS, OG_LB_MIN_BLOCKS) paired_kernel
 
     const uint32_t lane = blockIdx.x * blockDim.x + threadIdx.x;
     const size_t L = a.lanes_n;
-    const Sink sink{a.bitmap, a.bits, a.hits, a.counter, a.cap, a.search};
+    const Sink sink{a.bitmap, a.bits, a.hits, a.counter, a.cap, a.search, a.sbitmap, a.sbits};
     fe x = load_fe(a.lanes + 0 * L + lane, L);
     fe y = load_fe(a.lanes + 2 * L + lane, L);
     paired_rounds(x, y, words_fe(a.wx), words_fe(a.wy), words_fe(a.wt), qtab, a.half, a.rounds, a.scratch + lane, L,
@@ -65,7 +66,7 @@ __global__ void __launch_bounds__(OG_LB_THREADS, OG_LB_MIN_BLOCKS) paired_kernel
 __global__ void __launch_bounds__(OG_LB_THREADS, 5) chain_kernel(const ChainArgs a) {
     const uint32_t lane = blockIdx.x * blockDim.x + threadIdx.x;
     const size_t L = a.lanes_n;
-    const Sink sink{a.bitmap, a.bits, a.hits, a.counter, a.cap, a.search};
+    const Sink sink{a.bitmap, a.bits, a.hits, a.counter, a.cap, a.search, a.sbitmap, a.sbits};
     uint4* const scr = a.scratch + lane;
 #define SCR(e, w) (scr + ((size_t)(e) * 4 + (w) * 2) * L)
     fe X = load_fe(a.lanes + 0 * L + lane, L);
@@ -99,13 +100,71 @@ __global__ void __launch_bounds__(OG_LB_THREADS, 5) chain_kernel(const ChainArgs
     store_fe(a.lanes + 6 * L + lane, L, T);
 }
 
+// The filter a suffix-bitmap survivor matches, decided on its full address,
+// or 0xffffffff. Its key is recomputed from its offset: start + k 8G over
+// the binary expansion of k, then made affine; the recomputed y must equal
+// the survivor's (a mismatch is counted, never matched).
+__device__ __noinline__ uint32_t suffix_owner(const MatchArgs& a, const HitRec& r) {
+    const uint64_t w = a.window0 + (uint64_t)(r.step / a.slots) * a.lanes + r.lane;
+    const uint64_t k = w * a.slots + (a.paired ? 1u : 0u) + r.step % a.slots;
+    fe X = words_fe(a.sx), Y = words_fe(a.sy), Z = words_fe(a.sz), T = words_fe(a.st);
+#pragma unroll 1
+    for (uint32_t j = 0; j < 64; j++)
+        if ((k >> j) & 1) {
+            const uint4* p = a.pow8 + (size_t)j * 6;
+            add_cached(X, Y, Z, T, load_fe(p + 0, 1), load_fe(p + 2, 1), load_fe(p + 4, 1));
+        }
+    const fe zi = fe_invert(Z);
+    const fe x = fe_canon(fe_mulv(X, zi)), y = fe_canon(fe_mulv(Y, zi));
+    bool same = true;
+#pragma unroll
+    for (int q = 0; q < 8; q++) same &= y.v[q] == r.y[q];
+    if (!same) {
+        atomicAdd(a.mismatch, 1u);
+        return 0xffffffffu;
+    }
+    uint64_t pk[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) pk[q] = (uint64_t)y.v[2 * q] | ((uint64_t)y.v[2 * q + 1] << 32);
+    pk[3] |= (uint64_t)(x.v[0] & 1u) << 63;  // the sign bit
+    const uint32_t cs = onion_checksum(pk);
+    // pk || checksum || 0x03, and its base32 symbols (five bits each, most
+    // significant first)
+    uint8_t addr[36];
+#pragma unroll
+    for (int q = 0; q < 32; q++) addr[q] = (uint8_t)(pk[q / 8] >> (8 * (q % 8)));
+    addr[32] = (uint8_t)cs;
+    addr[33] = (uint8_t)(cs >> 8);
+    addr[34] = 0x03;
+    addr[35] = 0;
+    for (uint32_t j = 0; j < a.nsuffix; j++) {
+        const uint32_t* s = a.suffixes + (size_t)j * (MAX_SUFFIX_SYMBOLS + 1);
+        const uint32_t len = s[0], start = MAX_SUFFIX_SYMBOLS - len;
+        bool ok = true;
+        for (uint32_t i = 0; i < len && ok; i++) {
+            const uint32_t bit = (start + i) * 5, byte = bit / 8;
+            const uint32_t sym = ((((uint32_t)addr[byte] << 8) | addr[byte + 1]) >> (11 - bit % 8)) & 31u;
+            ok = (s[1 + i] >> sym) & 1u;
+        }
+        if (ok) return a.prefix_count + j;
+    }
+    return 0xffffffffu;
+}
+
 // Exact match of one advance's bitmap survivors (grid-stride; the survivor
 // count is read on the device, so the launch needs no host round trip).
-__global__ void __launch_bounds__(256) match_kernel(const MatchArgs a) {
+__global__ void __launch_bounds__(128) match_kernel(const MatchArgs a) {
     const uint32_t n = min(*a.surv_count, a.surv_cap);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const HitRec r = a.surv[i];
-        const uint32_t owner = exact_owner(a.t, r.y[0], r.y[1]);
+        uint32_t owner = a.t.nbuckets ? exact_owner(a.t, r.y[0], r.y[1]) : 0xffffffffu;
+        if (owner == 0xffffffffu && a.sbitmap) {
+            fe y;
+#pragma unroll
+            for (int q = 0; q < 8; q++) y.v[q] = r.y[q];
+            const uint32_t slot = suffix_slot(y, a.sbits);
+            if ((__ldg(a.sbitmap + (slot >> 5)) >> (slot & 31)) & 1u) owner = suffix_owner(a, r);
+        }
         if (owner != 0xffffffffu) {
             const uint32_t idx = atomicAdd(a.out_count, 1u);
             if (idx < a.out_cap) {
@@ -120,7 +179,7 @@ __global__ void __launch_bounds__(256) match_kernel(const MatchArgs a) {
 }  // namespace
 
 cudaError_t launch_match(const MatchArgs& a, int grid, cudaStream_t s) {
-    match_kernel<<<grid, 256, 0, s>>>(a);
+    match_kernel<<<grid, 128, 0, s>>>(a);
     return cudaGetLastError();
 }
 

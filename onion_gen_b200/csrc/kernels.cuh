@@ -48,12 +48,14 @@ struct PairedArgs {
     const uint4* table;      // Q_m, m = 1..half: ((m-1)*3 + {x,y,t}) * 2 + q
     uint4* lanes;            // affine centres: ({x,y} * 2 + q) * L + lane
     uint4* scratch;          // ((e * 2 + {num,den}) * 2 + q) * L + lane, e < 2 half + 2
-    const uint32_t* bitmap;  // prefix bitmap as 32-bit words; nullptr = every candidate survives
+    const uint32_t* bitmap;  // prefix bitmap as 32-bit words (nullptr: none)
     uint32_t bits;
     HitRec* hits;
     uint32_t* counter;
     uint32_t cap;
     uint32_t search;         // copied into every record
+    const uint32_t* sbitmap; // suffix bitmap (nullptr: none); with neither bitmap every candidate survives
+    uint32_t sbits;
     FeWords wx, wy, wt;      // the round stride W = L (2 half + 1) 8 G, affine
     uint32_t lanes_n;        // L, a multiple of the block size
     uint32_t half;
@@ -69,6 +71,8 @@ struct ChainArgs {
     uint32_t* counter;
     uint32_t cap;
     uint32_t search;
+    const uint32_t* sbitmap;
+    uint32_t sbits;
     FeWords step_ypx, step_ymx, step_t2d;  // +8G, Z = 1
     FeWords jump_ypx, jump_ymx, jump_t2d;  // +8 (L-1) n G, Z = 1 (unused when L = 1)
     uint32_t lanes_n;
@@ -106,14 +110,31 @@ struct MatchTables {
 
 // The single engine's exact match over one advance's bitmap survivors:
 // matching records are copied to `out` with `pad` = the filter's index.
+// Prefixes are matched on the key (MatchTables). A survivor whose slot is
+// set in the suffix bitmap has its full key recomputed from its offset
+// (start + k 8G), sign bit and checksum included, and is matched on its
+// address against every suffix.
+constexpr uint32_t MAX_SUFFIX_SYMBOLS = 56;
 struct MatchArgs {
     const HitRec* surv;
     const uint32_t* surv_count;
     uint32_t surv_cap;
-    MatchTables t;
+    MatchTables t;           // nbuckets = 0: no prefixes
+    const uint32_t* sbitmap; // suffix bitmap, nullptr: no suffixes
+    uint32_t sbits;
+    const uint32_t* suffixes;  // per suffix 57 words: its length, then one symbol set per position
+    uint32_t nsuffix;
+    uint32_t prefix_count;     // filter index of suffix j is prefix_count + j
+    FeWords sx, sy, sz, st;    // the engine's start point, extended
+    const uint4* pow8;         // 2^j 8G, j < 64, cached form: (j * 3 + {ypx,ymx,t2d}) * 2 + q
+    uint64_t window0;          // first window of the advance: launch * rounds * lanes
+    uint32_t lanes;
+    uint32_t slots;
+    uint32_t paired;           // offsets 8 (w slots + 1 + i), else 8 (w slots + i)
     HitRec* out;
     uint32_t* out_count;
     uint32_t out_cap;
+    uint32_t* mismatch;        // survivors whose recomputed key differs from their record
 };
 
 cudaError_t launch_init(const InitArgs& a, int block, cudaStream_t s);

@@ -30,7 +30,7 @@ __device__ __forceinline__ fe words_fe(const FeWords& w) {
     return r;
 }
 
-// Where survivors go: the bitmap, the record buffer and its counter.
+// Where survivors go: the bitmaps, the record buffer and its counter.
 struct Sink {
     const uint32_t* bitmap;
     uint32_t bits;
@@ -38,20 +38,42 @@ struct Sink {
     uint32_t* counter;
     uint32_t cap;
     uint32_t search;
+    const uint32_t* sbitmap;  // suffix bitmap, or nullptr
+    uint32_t sbits;
 };
 
-// Canonicalises y, tests its slot in the prefix bitmap and appends a record
-// for every lane of the warp that hit, with one atomic per warp. Every lane
-// of the warp must call this together (the kernels keep warps converged:
-// lane counts are whole blocks and loop trip counts are uniform).
+// Slot of a canonical key in the suffix bitmap: base32 bits
+// [255 - sbits, 255) of the packed key, i.e. bits 1..sbits of its last eight
+// bytes read big-endian (BitmapIndex::slot with offset 255 - sbits,
+// src/filter.rs:2536-2549). The sign bit (bit 7 of byte 31) is clear in the
+// packed key and the bitmap holds both of its values.
+__device__ __forceinline__ uint32_t suffix_slot(const fe& y, uint32_t sbits) {
+    const uint32_t lo = __byte_perm(y.v[7], 0, 0x0123), hi = __byte_perm(y.v[6], 0, 0x0123);
+    const uint32_t w = (lo >> 1) | (hi << 31);
+    return sbits >= 32 ? w : w & ((1u << sbits) - 1u);
+}
+
+// Canonicalises y, tests its slot in the prefix bitmap and in the suffix
+// bitmap (either lets it through; with neither, every candidate survives)
+// and appends a record for every lane of the warp that hit, with one atomic
+// per warp. Every lane of the warp must call this together (the kernels
+// keep warps converged: lane counts are whole blocks and loop trip counts
+// are uniform).
 __device__ __forceinline__ void test_emit(const Sink& k, const fe& yraw, uint32_t lane, uint32_t step) {
     const fe y = fe_canon(yraw);
     bool hit = true;
-    if (k.bitmap) {
-        // bytes 0..3 of the key, big-endian: the top of the slot
-        const uint32_t head = __byte_perm(y.v[0], 0, 0x0123);
-        const uint32_t slot = k.bits >= 32 ? head : head >> (32 - k.bits);
-        hit = (__ldg(k.bitmap + (slot >> 5)) >> (slot & 31)) & 1u;
+    if (k.bitmap || k.sbitmap) {
+        hit = false;
+        if (k.bitmap) {
+            // bytes 0..3 of the key, big-endian: the top of the slot
+            const uint32_t head = __byte_perm(y.v[0], 0, 0x0123);
+            const uint32_t slot = k.bits >= 32 ? head : head >> (32 - k.bits);
+            hit = (__ldg(k.bitmap + (slot >> 5)) >> (slot & 31)) & 1u;
+        }
+        if (k.sbitmap) {
+            const uint32_t slot = suffix_slot(y, k.sbits);
+            hit |= ((__ldg(k.sbitmap + (slot >> 5)) >> (slot & 31)) & 1u) != 0;
+        }
     }
     const unsigned mask = __ballot_sync(FULL, hit);
     if (mask == 0) return;

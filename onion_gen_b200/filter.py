@@ -1,9 +1,12 @@
-"""Literal-prefix filters (src/filter.rs), built by the engine's host code.
+"""Address filters (src/filter.rs), built by the engine's host code.
 
-``FilterSet.parse_all(["abc", "prefix:def"])`` sorts, drops absorbed filters,
-builds the prefix bitmap (width chosen as src/filter.rs:2279-2295 does unless
-``bits`` is given) and answers ``match_key`` exactly. Forms other than literal
-prefixes raise ``OgError`` (OG_E_FILTER).
+``FilterSet.parse_all(["abc", "prefix:def", "suffix:xyz2?[a-c]aad"])`` sorts,
+drops absorbed prefixes, builds the prefix bitmap (width chosen as
+src/filter.rs:2279-2295 does unless ``bits`` is given) and answers
+``match_key`` exactly for the prefixes. ``suffix:`` filters get their own
+bitmap keyed on the end of the key-derived span (src/filter.rs:2393-2480) and
+are decided on the full address (``match_address``). Other forms raise
+``OgError`` (OG_E_FILTER).
 """
 from __future__ import annotations
 
@@ -38,9 +41,9 @@ class FilterSet:
 
     def texts(self):
         out = []
-        b = C.create_string_buffer(64)
+        b = C.create_string_buffer(4096)
         for i in range(len(self)):
-            N.lib.og_filters_text(self._h, i, b, 64)
+            N.lib.og_filters_text(self._h, i, b, 4096)
             out.append(b.value.decode())
         return out
 
@@ -68,4 +71,22 @@ class FilterSet:
     def match_key(self, packed: bytes):
         """Index of the filter this packed key matches, or None."""
         i = N.lib.og_filters_match(self._h, bytes(packed))
+        return None if i < 0 else i
+
+    def prefix_count(self) -> int:
+        """Kept prefixes; filter indices at and above it are suffixes."""
+        return N.lib.og_filters_prefix_count(self._h)
+
+    def suffix_index_words(self):
+        """(words uint64[], bits) of the suffix bitmap; (empty, 0) without suffixes."""
+        p = C.POINTER(C.c_uint64)()
+        n = N.lib.og_filters_suffix_words(self._h, C.byref(p))
+        if n == 0:
+            return np.zeros(0, dtype=np.uint64), 0
+        return np.ctypeslib.as_array(p, shape=(n,)).copy(), N.lib.og_filters_suffix_bits(self._h)
+
+    def match_address(self, pk: bytes):
+        """The full check of a public key (sign bit included) on its address:
+        the index of the first filter it matches, or None."""
+        i = N.lib.og_filters_match_address(self._h, bytes(pk))
         return None if i < 0 else i

@@ -67,10 +67,14 @@ class Engine:
     ``start`` is the chain's first point as 128 bytes (X, Y, Z, T) — e.g.
     ``key.start_point(seed)``. ``threads=0`` takes the shape from tuning.yaml,
     or times the candidates and records the fastest. ``config`` (an
-    ``EngineConfig``) names an explicit shape instead.
+    ``EngineConfig``) names an explicit shape instead. ``filters`` (a
+    ``filter.FilterSet``, prefixes and suffixes) builds both bitmaps from the
+    set and turns the device match on (og_engine_new_filters); ``bitmap`` is
+    then ignored.
     """
 
-    def __init__(self, device=0, start=None, threads=0, bitmap=None, bitmap_bits=0, retune=False, config=None):
+    def __init__(self, device=0, start=None, threads=0, bitmap=None, bitmap_bits=0, retune=False, config=None,
+                 filters=None):
         ordinal = device.ordinal if isinstance(device, Device) else int(device)
         if start is None or len(start) != 128:
             raise ValueError("start must be a 128-byte point (X, Y, Z, T)")
@@ -78,7 +82,11 @@ class Engine:
         ptr = self._words.ctypes.data if self._words is not None else None
         h = C.c_void_p()
         err = N.errbuf()
-        if config is not None:
+        if filters is not None:
+            # og_engine_new_filters: both bitmaps from the set, device match on
+            cfgp = C.byref(config) if config is not None else None
+            rc = N.lib.og_engine_new_filters(ordinal, bytes(start), filters._h, cfgp, C.byref(h), err, 512)
+        elif config is not None:
             rc = N.lib.og_engine_new_config(
                 ordinal, bytes(start), C.byref(config), ptr, nwords, bitmap_bits, C.byref(h), err, 512
             )
@@ -90,6 +98,8 @@ class Engine:
         self._h = h
         self._room = N.lib.og_engine_room(h)
         self._buf = (N.Survivor * max(self._room, 1))()
+        if filters is not None:
+            self._mbuf = (N.Match * max(self._room, 1))()
 
     def close(self):
         if getattr(self, "_h", None):

@@ -16,6 +16,7 @@
 #define _GNU_SOURCE
 #include "oracle.h"
 
+#include <ctype.h>
 #include <math.h>
 #include <pthread.h>
 #include <stdio.h>
@@ -1345,4 +1346,277 @@ uint32_t orc_hit_room(uint64_t batch, uint32_t bits) {
     if (v < 4096) v = 4096;
     if (v > (1u << 18)) v = 1u << 18;
     return (uint32_t)v;
+}
+
+/* ========================================================================== */
+/* Suffix filters, src/filter.rs (the `suffix:` form)                          */
+/* ========================================================================== */
+
+#define ORC_ALL 0xffffffffu
+
+typedef struct {
+    uint32_t sets[56];
+    size_t len;
+    char text[64 * 34];
+} osuffix;
+
+struct orc_sset {
+    osuffix *p;
+    size_t n;
+    uint32_t bits;
+    uint64_t *words;
+    size_t nwords;
+};
+
+/* either_sign (src/filter.rs:158-164): symbol 49 holds the sign bit at
+ * weight 2, so each value pairs with the one two away in its group of four. */
+static uint32_t orc_either_sign(uint32_t set) {
+    uint32_t out = set;
+    for (unsigned v = 0; v < 32; v++)
+        if ((set >> v) & 1) out |= 1u << (v ^ 2);
+    return out;
+}
+
+/* symbol_at (src/filter.rs:259-267) over a buffer of `len` bytes. */
+static unsigned orc_symbol_at(const uint8_t *b, size_t len, size_t pos) {
+    unsigned v = 0;
+    for (unsigned k = 0; k < 5; k++) {
+        size_t bit = pos * 5 + k;
+        unsigned x = bit / 8 < len ? (b[bit / 8] >> (7 - bit % 8)) & 1 : 0;
+        v = (v << 1) | x;
+    }
+    return v;
+}
+
+/* Pattern::parse for a suffix body (src/filter.rs:298-350, parse_symbols
+ * :495-560, check_reachable_tail :566-600). */
+static int parse_suffix_body(const char *s, size_t len, osuffix *out, char *err, size_t errlen) {
+    size_t a = 0, b = len;
+    while (a < b && (s[a] == ' ' || s[a] == '\t' || s[a] == '\r')) a++;
+    while (b > a && (s[b - 1] == ' ' || s[b - 1] == '\t' || s[b - 1] == '\r')) b--;
+    memset(out, 0, sizeof *out);
+    size_t n = 0;
+    for (size_t i = a; i < b;) {
+        uint32_t set = 0;
+        if (s[i] == '?') {
+            set = ORC_ALL;
+            i++;
+        } else if (s[i] == '[') {
+            size_t e = i + 1;
+            while (e < b && s[e] != ']') e++;
+            if (e == b) { snprintf(err, errlen, "unbalanced class"); return -1; }
+            for (size_t j = i + 1; j < e;) {
+                int f = symbol_value((char)tolower((unsigned char)s[j]));
+                if (f < 0) { snprintf(err, errlen, "bad symbol"); return -1; }
+                if (j + 2 < e && s[j + 1] == '-') {
+                    int l = symbol_value((char)tolower((unsigned char)s[j + 2]));
+                    if (l < 0) { snprintf(err, errlen, "bad symbol"); return -1; }
+                    if (l < f) { snprintf(err, errlen, "empty range"); return -1; }
+                    for (int v = f; v <= l; v++) set |= 1u << v;
+                    j += 3;
+                } else {
+                    set |= 1u << f;
+                    j++;
+                }
+            }
+            if (!set) { snprintf(err, errlen, "empty class"); return -1; }
+            i = e + 1;
+        } else {
+            int v = symbol_value((char)tolower((unsigned char)s[i]));
+            if (v < 0) { snprintf(err, errlen, "bad symbol"); return -1; }
+            set = 1u << v;
+            i++;
+        }
+        if (n == 56) { snprintf(err, errlen, "too long"); return -1; }
+        out->sets[n++] = set;
+    }
+    if (n == 0) { snprintf(err, errlen, "empty"); return -1; }
+    int fixed = 0;
+    for (size_t i = 0; i < n; i++) fixed |= out->sets[i] != ORC_ALL;
+    if (!fixed) { snprintf(err, errlen, "nothing fixed"); return -1; }
+    if (!((out->sets[n - 1] >> symbol_value('d')) & 1)) { snprintf(err, errlen, "unreachable tail: last"); return -1; }
+    if (n >= 2) {
+        uint32_t tail = (1u << symbol_value('a')) | (1u << symbol_value('i')) | (1u << symbol_value('q')) |
+                        (1u << symbol_value('y'));
+        if (!(out->sets[n - 2] & tail)) { snprintf(err, errlen, "unreachable tail: penultimate"); return -1; }
+    }
+    out->len = n;
+    /* a text key for sorting and de-duplication */
+    size_t o = 0;
+    for (size_t i = 0; i < n; i++) {
+        if (out->sets[i] == ORC_ALL) {
+            out->text[o++] = '?';
+        } else if ((out->sets[i] & (out->sets[i] - 1)) == 0) {
+            out->text[o++] = B32[__builtin_ctz(out->sets[i])];
+        } else {
+            out->text[o++] = '[';
+            for (int v = 0; v < 32; v++)
+                if ((out->sets[i] >> v) & 1) out->text[o++] = B32[v];
+            out->text[o++] = ']';
+        }
+    }
+    out->text[o] = 0;
+    return 0;
+}
+
+static int cmp_suffix(const void *x, const void *y) {
+    return strcmp(((const osuffix *)x)->text, ((const osuffix *)y)->text);
+}
+
+/* suffix_slots (src/filter.rs:2438-2480): every slot of the window
+ * [255 - bits, 255) the suffix allows, built symbol by symbol; 0 when more
+ * than 4096. Returns the count, the slots in *out (malloc'd). */
+static size_t suffix_slot_list(const osuffix *p, uint32_t bits, uint32_t **out) {
+    size_t lo_bit = 255 - bits, hi_bit = 255, start = 56 - p->len;
+    uint32_t *vals = malloc(sizeof *vals);
+    size_t nv = 1;
+    vals[0] = 0;
+    for (size_t sym = lo_bit / 5; sym <= (hi_bit - 1) / 5; sym++) {
+        size_t lo = sym * 5 > lo_bit ? sym * 5 : lo_bit;
+        size_t hi = sym * 5 + 5 < hi_bit ? sym * 5 + 5 : hi_bit;
+        size_t width = hi - lo, shift = hi_bit - hi;
+        uint32_t set = sym >= start ? p->sets[sym - start] : ORC_ALL;
+        if (sym == 49) set = orc_either_sign(set);
+        uint32_t parts = 0; /* bitset of distinct parts (width <= 5) */
+        for (unsigned v = 0; v < 32; v++)
+            if ((set >> v) & 1) parts |= 1u << ((v >> (5 - (hi - sym * 5))) & ((1u << width) - 1));
+        size_t np = (size_t)__builtin_popcount(parts);
+        if (nv * np > 4096) {
+            free(vals);
+            *out = NULL;
+            return 0;
+        }
+        uint32_t *next = malloc(nv * np * sizeof *next);
+        size_t k = 0;
+        for (size_t i = 0; i < nv; i++)
+            for (unsigned part = 0; part < 32; part++)
+                if ((parts >> part) & 1) next[k++] = vals[i] | (part << shift);
+        free(vals);
+        vals = next;
+        nv = k;
+    }
+    *out = vals;
+    return nv;
+}
+
+static uint64_t *suffix_map(const osuffix *p, size_t n, uint32_t bits, size_t *nwords) {
+    size_t nw = (size_t)(((1ULL << bits) + 63) / 64);
+    uint64_t *w = calloc(nw, sizeof *w);
+    for (size_t i = 0; i < n; i++) {
+        uint32_t *sl;
+        size_t k = suffix_slot_list(&p[i], bits, &sl);
+        if (!k) {
+            free(w);
+            return NULL;
+        }
+        for (size_t j = 0; j < k; j++) w[sl[j] >> 6] |= 1ULL << (sl[j] & 63);
+        free(sl);
+    }
+    if (words_occupancy(w, nw, bits) > 0.25) {
+        free(w);
+        return NULL;
+    }
+    *nwords = nw;
+    return w;
+}
+
+orc_sset *orc_sset_new(const char *text, uint32_t bits, char *err, size_t errlen) {
+    size_t cap = 8, n = 0;
+    osuffix *p = malloc(cap * sizeof *p);
+    const char *q = text;
+    while (*q) {
+        const char *e = strchr(q, '\n');
+        size_t len = e ? (size_t)(e - q) : strlen(q);
+        int blank = 1;
+        for (size_t i = 0; i < len; i++)
+            if (q[i] != ' ' && q[i] != '\t' && q[i] != '\r') blank = 0;
+        if (!blank) {
+            if (n == cap) p = realloc(p, (cap *= 2) * sizeof *p);
+            if (parse_suffix_body(q, len, &p[n], err, errlen) != 0) {
+                free(p);
+                return NULL;
+            }
+            n++;
+        }
+        if (!e) break;
+        q = e + 1;
+    }
+    qsort(p, n, sizeof *p, cmp_suffix);
+    size_t kept = 0;
+    for (size_t i = 0; i < n; i++)
+        if (!kept || strcmp(p[i].text, p[kept - 1].text) != 0) p[kept++] = p[i];
+    orc_sset *s = calloc(1, sizeof *s);
+    s->p = p;
+    s->n = kept;
+    if (bits == 0) {
+        /* narrowest_acceptable(target_for_walk(n)) (src/filter.rs:2279-2300) */
+        double target = 0.01 / (double)(kept ? kept : 1);
+        for (uint32_t b = 16; b <= 24; b++) {
+            size_t nw;
+            uint64_t *w = suffix_map(p, kept, b, &nw);
+            if (!w) continue;
+            free(s->words);
+            s->words = w;
+            s->nwords = nw;
+            s->bits = b;
+            if (words_occupancy(w, nw, b) <= target) break;
+        }
+    } else {
+        s->words = suffix_map(p, kept, bits, &s->nwords);
+        s->bits = s->words ? bits : 0;
+    }
+    if (!s->words) {
+        snprintf(err, errlen, "no suffix index could be built");
+        orc_sset_free(s);
+        return NULL;
+    }
+    return s;
+}
+
+void orc_sset_free(orc_sset *s) {
+    if (!s) return;
+    free(s->p);
+    free(s->words);
+    free(s);
+}
+size_t orc_sset_count(const orc_sset *s) { return s->n; }
+uint32_t orc_sset_bits(const orc_sset *s) { return s->bits; }
+size_t orc_sset_nwords(const orc_sset *s) { return s->nwords; }
+const uint64_t *orc_sset_words(const orc_sset *s) { return s->words; }
+
+/* BitmapIndex::slot with offset 255 - bits (src/filter.rs:2536-2549). */
+int orc_sset_may_match(const orc_sset *s, const uint8_t packed[32]) {
+    uint32_t slot = 0;
+    for (uint32_t k = 0; k < s->bits; k++) {
+        uint32_t bit = 255 - s->bits + k;
+        slot = (slot << 1) | ((packed[bit / 8] >> (7 - bit % 8)) & 1);
+    }
+    return (int)((s->words[slot >> 6] >> (slot & 63)) & 1);
+}
+
+/* Filter::key_prefilter for a suffix (src/filter.rs:782-806). */
+int orc_sset_key_prefilter(const orc_sset *s, size_t i, const uint8_t packed[32]) {
+    const osuffix *p = &s->p[i];
+    size_t start = 56 - p->len;
+    for (size_t k = 0; k < p->len && start + k < 51; k++) {
+        uint32_t set = start + k == 49 ? orc_either_sign(p->sets[k]) : p->sets[k];
+        if (!((set >> orc_symbol_at(packed, 32, start + k)) & 1)) return 0;
+    }
+    return 1;
+}
+
+/* FilterSet::match_address over pk || checksum || 0x03 (src/filter.rs:2152). */
+long orc_sset_match_pk(const orc_sset *s, const uint8_t pk[32]) {
+    uint8_t a[35];
+    memcpy(a, pk, 32);
+    orc_checksum(pk, a + 32);
+    a[34] = 0x03;
+    for (size_t i = 0; i < s->n; i++) {
+        const osuffix *p = &s->p[i];
+        size_t start = 56 - p->len, k;
+        for (k = 0; k < p->len; k++)
+            if (!((p->sets[k] >> orc_symbol_at(a, 35, start + k)) & 1)) break;
+        if (k == p->len) return (long)i;
+    }
+    return -1;
 }

@@ -120,6 +120,25 @@ int orc_fset_may_match(const orc_fset *s, const uint8_t packed[32]);
 /* index of the first kept filter matching, or -1 (match_key). */
 long orc_fset_match(const orc_fset *s, const uint8_t packed[32]);
 
+/* ---- suffix filters, src/filter.rs (the `suffix:` form) ----------------- */
+typedef struct orc_sset orc_sset;
+/* newline-separated suffix bodies (without the "suffix:" form name): symbols,
+ * `?` and `[...]` classes; bits == 0 chooses the width the way
+ * FilterSet::with_index_bits does for suffixes. NULL and a message on a
+ * parse error or when no suffix index can be built. */
+orc_sset *orc_sset_new(const char *text, uint32_t bits, char *err, size_t errlen);
+void orc_sset_free(orc_sset *s);
+size_t orc_sset_count(const orc_sset *s);
+uint32_t orc_sset_bits(const orc_sset *s);
+size_t orc_sset_nwords(const orc_sset *s);
+const uint64_t *orc_sset_words(const orc_sset *s);
+/* the suffix index's bit test for a packed key (sign bit cleared). */
+int orc_sset_may_match(const orc_sset *s, const uint8_t packed[32]);
+/* Filter::key_prefilter of kept suffix i. */
+int orc_sset_key_prefilter(const orc_sset *s, size_t i, const uint8_t packed[32]);
+/* the first kept suffix the address of public key `pk` matches, or -1. */
+long orc_sset_match_pk(const orc_sset *s, const uint8_t pk[32]);
+
 /* ---- reference device bookkeeping --------------------------------------- */
 /* src/gpu/cuda.rs:332-354: scalar offset of (tid, slot) in launch `launch`
  * for `threads` threads and HALF = half. */

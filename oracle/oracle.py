@@ -53,6 +53,23 @@ def lib():
         L.orc_fset_may_match.argtypes = [P, U8P]
         L.orc_fset_match.restype = C.c_long
         L.orc_fset_match.argtypes = [P, U8P]
+        L.orc_sset_new.restype = P
+        L.orc_sset_new.argtypes = [U8P, U32, U8P, SZ]
+        L.orc_sset_free.argtypes = [P]
+        L.orc_sset_count.restype = SZ
+        L.orc_sset_count.argtypes = [P]
+        L.orc_sset_bits.restype = U32
+        L.orc_sset_bits.argtypes = [P]
+        L.orc_sset_nwords.restype = SZ
+        L.orc_sset_nwords.argtypes = [P]
+        L.orc_sset_words.restype = C.POINTER(U64)
+        L.orc_sset_words.argtypes = [P]
+        L.orc_sset_may_match.restype = C.c_int
+        L.orc_sset_may_match.argtypes = [P, U8P]
+        L.orc_sset_key_prefilter.restype = C.c_int
+        L.orc_sset_key_prefilter.argtypes = [P, SZ, U8P]
+        L.orc_sset_match_pk.restype = C.c_long
+        L.orc_sset_match_pk.argtypes = [P, U8P]
         L.orc_cuda_offset.restype = U64
         L.orc_cuda_offset.argtypes = [U64, U64, U64, U32, U32]
         L.orc_hit_room.restype = U32
@@ -322,3 +339,43 @@ class FilterSet:
 
     def match(self, packed: bytes) -> int:
         return lib().orc_fset_match(self._h, packed)
+
+
+class SuffixSet:
+    """Suffix filters (the `suffix:` form) with their suffix bitmap."""
+
+    def __init__(self, bodies, bits: int = 0):
+        err = _buf(256)
+        text = "\n".join(bodies).encode()
+        self._h = lib().orc_sset_new(text, bits, err, 256)
+        if not self._h:
+            raise ValueError(err.value.decode())
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().orc_sset_free(h)
+            self._h = None
+
+    def __len__(self):
+        return lib().orc_sset_count(self._h)
+
+    @property
+    def bits(self) -> int:
+        return lib().orc_sset_bits(self._h)
+
+    def words(self):
+        import numpy as np
+
+        n = lib().orc_sset_nwords(self._h)
+        p = lib().orc_sset_words(self._h)
+        return np.ctypeslib.as_array(p, shape=(n,)).copy()
+
+    def may_match(self, packed: bytes) -> bool:
+        return bool(lib().orc_sset_may_match(self._h, packed))
+
+    def key_prefilter(self, i: int, packed: bytes) -> bool:
+        return bool(lib().orc_sset_key_prefilter(self._h, i, packed))
+
+    def match_pk(self, pk: bytes) -> int:
+        return lib().orc_sset_match_pk(self._h, pk)

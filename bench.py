@@ -20,6 +20,9 @@ One JSON line on rank 0:
   cpu_baseline the oracle's restatement of the reference's paired CPU engine
               (src/pairs.rs, batch 8192 as src/run.rs uses) on every host core
 
+  batch_shape the batch's autotuner (og_batch_tune): inversion batch,
+              slot pool and grid, the fastest within 20 ms a step; the
+              batched and serving legs run that shape
   batched     config 4 (64 searches, 1..5000 prefixes of 4..7 symbols, quota
               1..16): the single-search engine one search at a time (the
               run driver's loop) against the batched engine, same results;
@@ -50,8 +53,11 @@ sys.path.insert(0, ROOT)
 
 CANDIDATES_PER_STEP = 1 << 32
 HALF = 1024
-# the batched engine keeps rounds short: a step is one round of every lane
-BATCH_HALF = 256
+# the plain engine of the batched leg (one search at a time) and the batch's
+# profiling case: a short round, so that small searches do not overshoot
+SHORT_HALF = 256
+# the batch's shape comes from its autotuner, within this much device time a step
+BATCH_STEP_CAP_MS = 20.0
 CPU_HALF = 4096  # PairEngine::new(8192) (src/run.rs:601, src/batch.rs:32)
 # DRAM bytes per candidate of paired_kernel, from one ncu capture of one
 # launch at the plain line's shape (half 1024, 227,328 lanes:
@@ -75,7 +81,7 @@ def parse():
                    "batch-small: three steps of the batched engine over the first 16 config-4 searches")
     p.add_argument("--half", type=int, default=0,
                    help=f"inversion batch half-width (default {HALF} for the plain line, 256 for --case small, "
-                   f"{BATCH_HALF} for the batched engine)")
+                   f"{SHORT_HALF} for the batch's profiling case)")
     p.add_argument("--suite", default="default", choices=["default", "batched", "serving", "plain"],
                    help="default: the plain line plus bounded batched and serving legs; "
                    "batched / serving: that leg at full size; plain: the plain line only")
@@ -221,7 +227,20 @@ def log(msg):
     print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
 
 
-def batched_leg(dev, half, cap):
+def batch_shape(dev):
+    """The batch's autotuner (og_batch_tune): inversion batch, slot pool and
+    grid, the fastest within BATCH_STEP_CAP_MS of device time a step."""
+    from onion_gen_b200 import batch as B
+
+    t0 = time.perf_counter()
+    cfg, rate = B.tune(dev, 64, BATCH_STEP_CAP_MS)
+    shape = {"half": cfg.half, "slots": cfg.slots, "grid": cfg.grid, "rounds": cfg.rounds}
+    log(f"batch tuner: {shape} at {rate:.4e} keys/s in {time.perf_counter() - t0:.1f} s")
+    return shape, {**shape, "tuned_keys_per_s": rate, "step_cap_ms": BATCH_STEP_CAP_MS,
+                   "tune_s": time.perf_counter() - t0}
+
+
+def batched_leg(dev, shape, cap):
     """Config 4: plain (one engine per search) against batched, same searches."""
     from onion_gen_b200 import _native as N
     from onion_gen_b200 import batch as B
@@ -229,7 +248,7 @@ def batched_leg(dev, half, cap):
 
     all_searches = workloads.config4_searches()
     searches = [s for s in all_searches if s.expected_candidates() <= cap]
-    cfg = N.EngineConfig(N.SCHEME_PAIRED, half, 0, 0, 128, 0, 0)
+    cfg = N.EngineConfig(N.SCHEME_PAIRED, SHORT_HALF, 0, 0, 128, 0, 0)
     t0 = time.perf_counter()
     plain, plain_examined, plain_launches = {}, 0, 0
     for s in searches:
@@ -241,7 +260,7 @@ def batched_leg(dev, half, cap):
     log(f"batched leg: plain engine {len(searches)} searches in {plain_wall:.2f} s")
 
     t0 = time.perf_counter()
-    b = B.Batch(dev, half=half)
+    b = B.Batch(dev, **shape)
     for s in searches:
         b.admit(s.index, s.seed, s.prefixes, s.quota)
     steps = launches = 0
@@ -276,12 +295,12 @@ def batched_leg(dev, half, cap):
     }
 
 
-def serving_leg(dev, half, n, cap_s):
+def serving_leg(dev, shape, n, cap_s):
     """Config 5: requests submitted at their Poisson arrival times."""
     from onion_gen_b200 import serve, workloads
 
     reqs = workloads.config5_requests(n)
-    s = serve.Server(dev, half=half)
+    s = serve.Server(dev, **shape)
     t0 = s.now_ns()
     submitted = 0
     done = {}
@@ -360,7 +379,7 @@ def batch_small_case(args):
     from onion_gen_b200 import gpu, workloads
 
     dev = gpu.look()[0]
-    b = B.Batch(dev, half=args.half or BATCH_HALF)
+    b = B.Batch(dev, half=args.half or SHORT_HALF)
     for s in workloads.config4_searches()[:16]:
         b.admit(s.index, s.seed, s.prefixes, s.quota)
     for i in range(3):
@@ -555,13 +574,15 @@ def main():
         if e2e:
             line["e2e"] = e2e
         line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+        if args.suite in ("default", "batched", "serving"):
+            shape, line["batch_shape"] = batch_shape(dev)
         if args.suite in ("default", "batched"):
             cap = args.batched_cap if args.suite == "default" else float("inf")
-            line["batched"] = batched_leg(dev, BATCH_HALF, cap)
+            line["batched"] = batched_leg(dev, shape, cap)
         if args.suite in ("default", "serving"):
             n = args.serving_requests if args.suite == "default" else 2000
             cap = args.serving_cap if args.suite == "default" else 120.0
-            line["serving"] = serving_leg(dev, BATCH_HALF, n, cap)
+            line["serving"] = serving_leg(dev, shape, n, cap)
         print(json.dumps(line), flush=True)
     if pg:
         pg.destroy_process_group()

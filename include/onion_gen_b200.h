@@ -182,6 +182,7 @@ typedef struct og_batch_config {
     uint32_t max_searches;  /* searches admitted at once (0: 4096) */
     uint32_t max_hits;      /* exact hits one step may return (0: 65536) */
     uint32_t graph;         /* 0 or 1: replay each step as a captured CUDA graph; 2: plain launches */
+    uint32_t grid;          /* persistent CTAs per SM (0: as many as fit) */
     uint64_t memory_budget; /* device bytes for per-search tables (0: half of the free memory after the pool) */
 } og_batch_config;
 
@@ -206,6 +207,20 @@ typedef struct og_search_status {
 } og_search_status;
 
 int og_batch_new(int ordinal, const og_batch_config* cfg, og_batch** out, char* err, size_t errlen);
+
+/* The batch's autotuner. Times a synthetic mix of `searches` searches (0:
+ * 64) that never reach their quota at every shape of inversion batch (half
+ * 128, 256, 512), slot pool (1, 2, 3 waves of persistent CTAs) and grid
+ * (all resident CTAs per SM, or half of them), keeps the highest keys/s
+ * whose step stays within `max_step_ms` of device time (0: no cap),
+ * records it in tuning.yaml under `device/<name>/cuda-batch/0/<version>`
+ * (first = half, second = slots, block = grid, rounds) and writes it to
+ * `out` (other fields zero: defaults). og_batch_new takes the recorded
+ * shape when half, slots, rounds and grid are all 0. */
+int og_batch_tune(int ordinal, uint32_t searches, float max_step_ms, og_batch_config* out, double* keys_per_s,
+                  char* err, size_t errlen);
+/* The shape a batch runs (defaults filled in). */
+void og_batch_shape(const og_batch* b, og_batch_config* cfg);
 /* Admits a search: `filters` newline-separated literal prefixes. Fails with
  * OG_E_NOMEM when its tables do not fit the memory budget (nothing is
  * changed), OG_E_CAPACITY when max_searches are admitted. */

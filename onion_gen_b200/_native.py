@@ -66,6 +66,7 @@ class BatchConfig(C.Structure):
         ("max_searches", C.c_uint32),
         ("max_hits", C.c_uint32),
         ("graph", C.c_uint32),
+        ("grid", C.c_uint32),
         ("memory_budget", C.c_uint64),
     ]
 
@@ -155,6 +156,8 @@ def _load():
     sig("og_engine_free", None, [P])
     sig("og_batch_new", I, [I, C.POINTER(BatchConfig), C.POINTER(P), B, SZ])
     sig("og_batch_admit", I, [P, U64, B, B, U32, B, SZ])
+    sig("og_batch_tune", I, [I, U32, C.c_float, C.POINTER(BatchConfig), C.POINTER(C.c_double), B, SZ])
+    sig("og_batch_shape", None, [P, C.POINTER(BatchConfig)])
     sig("og_batch_step", I, [P, P, SZ, C.POINTER(SZ), B, SZ])
     sig("og_batch_room", SZ, [P])
     sig("og_batch_status", I, [P, U64, C.POINTER(SearchStatus)])

@@ -33,9 +33,10 @@ def _hit(h: N.BatchHit) -> Hit:
 
 
 class Batch:
-    def __init__(self, device=0, half=0, slots=0, rounds=0, max_searches=0, max_hits=0, graph=True, memory_budget=0):
+    def __init__(self, device=0, half=0, slots=0, rounds=0, max_searches=0, max_hits=0, graph=True, memory_budget=0,
+                 grid=0):
         ordinal = getattr(device, "ordinal", device)
-        cfg = N.BatchConfig(half, slots, rounds, max_searches, max_hits, 1 if graph else 2, memory_budget)
+        cfg = N.BatchConfig(half, slots, rounds, max_searches, max_hits, 1 if graph else 2, grid, memory_budget)
         h = C.c_void_p()
         err = N.errbuf()
         N.check(N.lib.og_batch_new(int(ordinal), C.byref(cfg), C.byref(h), err, 512), err)
@@ -55,6 +56,11 @@ class Batch:
 
     def __exit__(self, *a):
         self.close()
+
+    def shape(self) -> N.BatchConfig:
+        c = N.BatchConfig()
+        N.lib.og_batch_shape(self._h, C.byref(c))
+        return c
 
     def admit(self, search_id: int, seed: bytes, prefixes, quota: int) -> None:
         err = N.errbuf()
@@ -109,3 +115,16 @@ class Batch:
         u, b = C.c_uint64(), C.c_uint64()
         N.lib.og_batch_memory(self._h, C.byref(u), C.byref(b))
         return u.value, b.value
+
+
+def tune(device=0, searches: int = 0, max_step_ms: float = 0.0):
+    """og_batch_tune: times the batch over inversion batch, slot pool and grid,
+    records the fastest shape (within ``max_step_ms`` of device time a step)
+    in tuning.yaml and returns (BatchConfig, keys/s). A Batch created with
+    half, slots, rounds and grid all 0 then runs that shape."""
+    ordinal = getattr(device, "ordinal", device)
+    cfg = N.BatchConfig()
+    rate = C.c_double()
+    err = N.errbuf()
+    N.check(N.lib.og_batch_tune(int(ordinal), searches, max_step_ms, C.byref(cfg), C.byref(rate), err, 512), err)
+    return cfg, rate.value

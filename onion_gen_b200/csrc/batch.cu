@@ -32,6 +32,7 @@
 #include "host/common.h"
 #include "host/filters.h"
 #include "host/keys.h"
+#include "host/tuning.h"
 #include "search_common.cuh"
 
 #ifndef OG_LB_THREADS
@@ -158,6 +159,14 @@ __global__ void __launch_bounds__(256) batch_exact_kernel(const BatchArgs a) {
             }
         }
     }
+}
+
+// The tuning.yaml key of the batch's shape on a device.
+std::string batch_key(int ordinal) {
+    char name[256] = "unnamed";
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, ordinal) == cudaSuccess) snprintf(name, sizeof name, "%s", p.name);
+    return device_key(name, "cuda-batch", 0);
 }
 
 struct Search {
@@ -344,6 +353,16 @@ int og_batch_new(int ordinal, const og_batch_config* cfgp, og_batch** out, char*
     if (ordinal < 0 || ordinal >= count) return fail(err, errlen, OG_E_ARG, "device %d of %d", ordinal, count);
     og_batch_config cfg{};
     if (cfgp) cfg = *cfgp;
+    if (cfg.half == 0 && cfg.slots == 0 && cfg.rounds == 0 && cfg.grid == 0) {
+        // the shape og_batch_tune recorded for this device, if any
+        Shape s;
+        if (tuning_get(batch_key(ordinal), s) && s.first && s.second) {
+            cfg.half = s.first;
+            cfg.slots = s.second;
+            cfg.grid = s.block;
+            cfg.rounds = s.rounds;
+        }
+    }
     if (cfg.half == 0) cfg.half = 256;
     if (cfg.half > 2048) return fail(err, errlen, OG_E_ARG, "half %u > 2048", cfg.half);
     if (cfg.rounds == 0) cfg.rounds = 1;
@@ -357,7 +376,9 @@ int og_batch_new(int ordinal, const og_batch_config* cfgp, og_batch** out, char*
     int per_sm = 0, sms = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_search_kernel, BLOCK, b->smem));
     CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ordinal));
-    b->grid = (uint32_t)std::max(1, per_sm) * (uint32_t)sms;
+    const uint32_t fit = (uint32_t)std::max(1, per_sm);
+    cfg.grid = cfg.grid == 0 ? fit : std::min(cfg.grid, fit);
+    b->grid = cfg.grid * (uint32_t)sms;
     if (cfg.slots == 0) cfg.slots = 2 * b->grid * BLOCK;
     cfg.slots = (cfg.slots + BLOCK - 1) / BLOCK * BLOCK;
     b->slots = cfg.slots;
@@ -707,6 +728,93 @@ uint32_t og_batch_last_step_launches(const og_batch* b) { return b ? b->last_lau
 void og_batch_memory(const og_batch* b, uint64_t* used, uint64_t* budget) {
     if (used) *used = b ? b->mem_used : 0;
     if (budget) *budget = b ? b->mem_budget : 0;
+}
+
+void og_batch_shape(const og_batch* b, og_batch_config* cfg) {
+    if (b && cfg) *cfg = b->cfg;
+}
+
+int og_batch_tune(int ordinal, uint32_t searches, float max_step_ms, og_batch_config* out, double* keys_per_s,
+                  char* err, size_t errlen) {
+    if (!out) return fail(err, errlen, OG_E_ARG, "null argument");
+    if (searches == 0) searches = 64;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+        return fail(err, errlen, OG_E_NODEVICE, "no CUDA device is available");
+    if (ordinal < 0 || ordinal >= count) return fail(err, errlen, OG_E_ARG, "device %d of %d", ordinal, count);
+    CU(cudaSetDevice(ordinal));
+    int per_sm = 0, sms = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_search_kernel, BLOCK, 0));
+    CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ordinal));
+    const uint32_t fit = (uint32_t)std::max(1, per_sm);
+    // a mix that never finishes: each search one ten-symbol prefix (50 bits)
+    std::vector<std::string> prefixes(searches);
+    for (uint32_t j = 0; j < searches; j++) {
+        std::string p;
+        uint32_t v = j * 2654435761u + 12345u;
+        for (int k = 0; k < 10; k++) {
+            p.push_back(BASE32_ALPHABET[v & 31]);
+            v = v * 1103515245u + 12345u;
+        }
+        prefixes[j] = p;
+    }
+    og_batch_config best{};
+    double best_rate = -1;
+    int last = OG_E_DEVICE;
+    for (uint32_t half : {128u, 256u, 512u}) {
+        for (uint32_t grid : {fit, std::max(1u, fit / 2)}) {
+            for (uint32_t waves : {1u, 2u, 3u}) {
+                og_batch_config c{};
+                c.half = half;
+                c.grid = grid;
+                c.slots = waves * grid * (uint32_t)sms * BLOCK;
+                c.rounds = 1;
+                c.max_searches = searches;
+                c.graph = 1;
+                og_batch* b = nullptr;
+                last = og_batch_new(ordinal, &c, &b, err, errlen);
+                if (last != OG_OK) continue;
+                for (uint32_t j = 0; j < searches && last == OG_OK; j++) {
+                    uint8_t seed[32] = {0};
+                    const uint32_t id = 0x7f000000u + j;
+                    std::memcpy(seed, &id, 4);
+                    last = og_batch_admit(b, j, seed, prefixes[j].c_str(), 1, err, errlen);
+                }
+                double ms = 0, cand = 0;
+                for (int step = 0; step < 6 && last == OG_OK; step++) {
+                    size_t n = 0;
+                    last = og_batch_step(b, nullptr, 0, &n, err, errlen);
+                    if (step >= 2) {
+                        ms += og_batch_last_step_ms(b);
+                        cand += (double)og_batch_last_step_candidates(b);
+                    }
+                }
+                og_batch_free(b);
+                if (last != OG_OK || ms <= 0) continue;
+                const double rate = cand / (ms * 1e-3);
+                if ((max_step_ms <= 0 || ms / 4 <= max_step_ms) && rate > best_rate) {
+                    best_rate = rate;
+                    best = og_batch_config{};
+                    best.half = half;
+                    best.slots = c.slots;
+                    best.rounds = 1;
+                    best.grid = grid;
+                }
+            }
+        }
+    }
+    if (best_rate < 0) return fail(err, errlen, last, "no batch shape ran within %.1f ms a step", max_step_ms);
+    Shape s;
+    s.first = best.half;
+    s.second = best.slots;
+    s.block = best.grid;
+    s.rounds = best.rounds;
+    s.rate = best_rate;
+    s.at = unix_now();
+    tuning_put(batch_key(ordinal), s);
+    *out = best;
+    if (keys_per_s) *keys_per_s = best_rate;
+    return OG_OK;
 }
 
 void og_batch_free(og_batch* b) { delete b; }

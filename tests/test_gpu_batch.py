@@ -144,3 +144,22 @@ def test_retire_mid_search_and_errors(device):
     while b.running():
         b.step()
     assert len(b.results(8)) == 2
+
+
+def test_tuner_records_a_shape_that_finds_the_same_hits(device, mixed, tmp_path, monkeypatch):
+    """og_batch_tune walks inversion batch, slot pool and grid, records the
+    fastest shape in tuning.yaml, and a batch created with zeros runs it; the
+    hits of a search do not depend on the shape."""
+    monkeypatch.setenv("ONION_GEN_TUNING_FILE", str(tmp_path / "tuning.yaml"))
+    cfg, rate = B.tune(device, searches=16, max_step_ms=50.0)
+    assert rate > 1e9
+    assert cfg.half in (128, 256, 512) and cfg.slots % 128 == 0 and cfg.grid >= 1
+    text = (tmp_path / "tuning.yaml").read_text()
+    assert f"device/{device.name}/cuda-batch/0/" in text
+    b = B.Batch(device)
+    shape = b.shape()
+    assert (shape.half, shape.slots, shape.grid, shape.rounds) == (cfg.half, cfg.slots, cfg.grid, cfg.rounds)
+    b.close()
+    out, _ = mixed
+    tuned, _ = run_batch(device, SEARCHES, half=0, slots=0)
+    assert tuned == out

@@ -21,7 +21,7 @@ One JSON line on rank 0:
               (src/pairs.rs, batch 8192 as src/run.rs uses) on every host core
 
   batch_shape the batch's autotuner (og_batch_tune): inversion batch,
-              slot pool and grid, the fastest within 20 ms a step; the
+              slot pool and grid, the fastest within 8 ms a step; the
               batched and serving legs run that shape
   batched     config 4 (64 searches, 1..5000 prefixes of 4..7 symbols, quota
               1..16): the single-search engine one search at a time (the
@@ -57,7 +57,7 @@ HALF = 1024
 # profiling case: a short round, so that small searches do not overshoot
 SHORT_HALF = 256
 # the batch's shape comes from its autotuner, within this much device time a step
-BATCH_STEP_CAP_MS = 20.0
+BATCH_STEP_CAP_MS = 8.0
 CPU_HALF = 4096  # PairEngine::new(8192) (src/run.rs:601, src/batch.rs:32)
 # DRAM bytes per candidate of paired_kernel, from one ncu capture of one
 # launch at the plain line's shape (half 1024, 227,328 lanes:

@@ -60,7 +60,17 @@ __device__ __forceinline__ uint32_t suffix_slot(const fe& y, uint32_t sbits) {
 // keep warps converged: lane counts are whole blocks and loop trip counts
 // are uniform).
 __device__ __forceinline__ void test_emit(const Sink& k, const fe& yraw, uint32_t lane, uint32_t step) {
-    const fe y = fe_canon(yraw);
+    // The canonical limbs the bitmaps read (0, 6 and 7), without the full
+    // canonicalisation. Folding bit 255 adds 19 to limb 0; its carry reaches
+    // limb 6 only through limbs 1..5 all ones, and the value can be p or
+    // more only with limbs 1..6 all ones (a carry out of limb 0 leaves it
+    // below 19, too small for that). Outside that case, which a uniform key
+    // meets with probability 2^-160, the canonical limbs are these.
+    fe y;
+    y.v[0] = yraw.v[0] + ((yraw.v[7] >> 31) ? 19u : 0u);
+    y.v[6] = yraw.v[6];
+    y.v[7] = yraw.v[7] & 0x7fffffffu;
+    if ((yraw.v[1] & yraw.v[2] & yraw.v[3] & yraw.v[4] & yraw.v[5]) == 0xffffffffu) y = fe_canon(yraw);
     bool hit = true;
     if (k.bitmap || k.sbitmap) {
         hit = false;
@@ -85,6 +95,7 @@ __device__ __forceinline__ void test_emit(const Sink& k, const fe& yraw, uint32_
     if (hit) {
         const uint32_t idx = base + (uint32_t)__popc(mask & ((1u << me) - 1u));
         if (idx < k.cap) {
+            y = fe_canon(yraw);
             uint4* rec = reinterpret_cast<uint4*>(k.hits + idx);
             rec[0] = make_uint4(lane, step, k.search, 0u);
             rec[1] = make_uint4(y.v[0], y.v[1], y.v[2], y.v[3]);

@@ -20,6 +20,10 @@ One JSON line on rank 0:
   cpu_baseline the oracle's restatement of the reference's paired CPU engine
               (src/pairs.rs, batch 8192 as src/run.rs uses) on every host core
 
+  suffix      a suffix search (16 suffixes of 9 symbols) through the filter
+              engine: suffix bitmap in the search kernel, full key, sign bit
+              and SHA3-256 checksum recomputed on the device for its
+              survivors, every match re-derived on the host
   batch_shape the batch's autotuner (og_batch_tune): inversion batch,
               slot pool and grid, the fastest within 8 ms a step; the
               batched and serving legs run that shape
@@ -76,15 +80,16 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--case", default="full", choices=["full", "small", "batch-small"],
+    p.add_argument("--case", default="full", choices=["full", "small", "batch-small", "suffix-small"],
                    help="small: the profiling case, three one-round advances of the plain engine; "
-                   "batch-small: three steps of the batched engine over the first 16 config-4 searches")
+                   "batch-small: three steps of the batched engine over the first 16 config-4 searches; "
+                   "suffix-small: three advances of a forty-suffix search with the device match")
     p.add_argument("--half", type=int, default=0,
                    help=f"inversion batch half-width (default {HALF} for the plain line, 256 for --case small, "
                    f"{SHORT_HALF} for the batch's profiling case)")
-    p.add_argument("--suite", default="default", choices=["default", "batched", "serving", "plain"],
-                   help="default: the plain line plus bounded batched and serving legs; "
-                   "batched / serving: that leg at full size; plain: the plain line only")
+    p.add_argument("--suite", default="default", choices=["default", "batched", "serving", "plain", "suffix"],
+                   help="default: the plain line plus bounded suffix, batched and serving legs; "
+                   "batched / serving / suffix: that leg at full size; plain: the plain line only")
     p.add_argument("--batched-cap", type=float, default=2e10,
                    help="largest expected work (candidates) of a config-4 search in the default run")
     p.add_argument("--serving-requests", type=int, default=400)
@@ -372,6 +377,68 @@ def small_case(args):
               f"{eng.batch() / ms * 1e3:.4e} keys/s")
 
 
+def suffix_small_case(args):
+    """Three advances of a suffix search (og_engine_new_filters, forty
+    eight-symbol suffixes, half 256, one resident wave): the case the suffix
+    match kernel's ncu summary is captured on."""
+    from onion_gen_b200 import _native as N
+    from onion_gen_b200 import filter as F
+    from onion_gen_b200 import gpu, key, workloads
+
+    dev = gpu.look()[0]
+    fs = F.FilterSet.parse_all(workloads.suffix_filters(40, 8))
+    start = key.start_point(workloads.seed(0))
+    lanes = dev.sms * 6 * 128
+    eng = gpu.Engine(dev, start, filters=fs, config=N.EngineConfig(0, args.half or 256, lanes, 1, 128, 0, 0))
+    for i in range(3):
+        o, _, _ = eng.advance_matches_raw()
+        print(f"advance {i}: {len(o)} matches, search kernel {eng.last_kernel_ms():.3f} ms")
+
+
+def suffix_leg(dev, steps, advances):
+    """A suffix search through the filter engine (og_engine_new_filters +
+    og_engine_advance_matches): the search kernel with the suffix bitmap, the
+    device match (full key, sign bit and SHA3-256 checksum recomputed for each
+    suffix survivor) and the host's re-derivation of every match."""
+    from onion_gen_b200 import _native as N
+    from onion_gen_b200 import filter as F
+    from onion_gen_b200 import gpu, key, workloads
+
+    suffixes = workloads.suffix_filters()
+    fs = F.FilterSet.parse_all(suffixes)
+    seed = workloads.seed(0)
+    eng = gpu.Engine(dev, key.start_point(seed), filters=fs,
+                     config=N.EngineConfig(N.SCHEME_PAIRED, HALF, 0, 0, 128, 0, 0))
+    eng.advance_matches_raw()
+    texts = fs.texts()
+    matches = verified = 0
+    kernel_ms = 0.0
+    t0 = time.perf_counter()
+    for _ in range(steps * advances):
+        o, k, f = eng.advance_matches_raw()
+        kernel_ms += eng.last_kernel_ms()
+        for off, packed, fi in zip(o, k, f):
+            pk, _ = key.check_hit(seed, int(off), bytes(packed))
+            matches += 1
+            verified += fs.match_address(pk) == int(fi) and texts[int(fi)].startswith("suffix:")
+    wall = time.perf_counter() - t0
+    n = eng.batch() * steps * advances
+    eng.close()
+    sb = fs.suffix_index_words()[1]
+    log(f"suffix leg: {n:.3e} candidates in {wall:.2f} s, {matches} matches")
+    return {
+        "workload": "suffix search: seed LE32(0), 16 suffixes of 9 symbols (splitmix64(6)), "
+        f"suffix bitmap {sb} bits, {steps} steps of {advances} advances",
+        "candidates": n,
+        "keys_per_s": n / wall,
+        "search_kernel_keys_per_s": n / (kernel_ms * 1e-3),
+        "matches": matches,
+        "matches_verified": verified,
+        "expected_matches": n * len(suffixes) * 2.0 ** -37,
+        "unit": "keys/s (wall clock, device match and host re-derivation included)",
+    }
+
+
 def batch_small_case(args):
     """Three steps of the batched engine with the first 16 config-4 searches
     admitted: the case the batched kernels' ncu summaries are captured on."""
@@ -399,6 +466,9 @@ def main():
         return
     if args.case == "batch-small":
         batch_small_case(args)
+        return
+    if args.case == "suffix-small":
+        suffix_small_case(args)
         return
     rank, world, local = dist_env()
     import ctypes as C
@@ -574,6 +644,8 @@ def main():
         if e2e:
             line["e2e"] = e2e
         line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+        if args.suite in ("default", "suffix"):
+            line["suffix"] = suffix_leg(dev, 2 if args.suite == "default" else args.steps, advances)
         if args.suite in ("default", "batched", "serving"):
             shape, line["batch_shape"] = batch_shape(dev)
         if args.suite in ("default", "batched"):

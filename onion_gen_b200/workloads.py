@@ -107,3 +107,14 @@ def config5_requests(n: int = 2000, rate: float = 50.0):
         quota = 1 + r.next() % 16
         out.append(Search(j, seed(j), prefixes, quota, arrival=t))
     return out
+
+
+def suffix_filters(n: int = 16, length: int = 9):
+    """A suffix workload: `n` suffixes of `length` symbols from splitmix64(6),
+    each ending in a reachable v3 tail (a symbol of "aiqy", then "d")."""
+    rng = SplitMix64(6)
+    out = []
+    for _ in range(n):
+        body = "".join(ALPHABET[rng.next() % 32] for _ in range(length - 2))
+        out.append("suffix:" + body + "aiqy"[rng.next() % 4] + "d")
+    return out

@@ -34,6 +34,7 @@
 #include "host/keys.h"
 #include "host/tuning.h"
 #include "search_common.cuh"
+#include "suffix_match.cuh"
 
 #ifndef OG_LB_THREADS
 #define OG_LB_THREADS 128
@@ -62,9 +63,23 @@ constexpr double MAX_OCCUPANCY = 0.02;
 struct BatchDesc {
     FeWords wx, wy, wt;      // the search's stride for this step: L (2 half + 1) 8 G, affine
     FeWords bx, by, bz, bt;  // centre of window W_done (where new lanes start), extended
-    const uint32_t* bitmap;
+    const uint32_t* bitmap;  // prefix bitmap (nullptr: the search has no prefix)
     uint32_t bits;
     MatchTables match;
+    const uint32_t* sbitmap;  // suffix bitmap (nullptr: no suffix)
+    uint32_t sbits;
+    uint32_t prefix_count;    // filter index of suffix j is prefix_count + j
+    const uint32_t* suffixes; // the suffix patterns (SuffixTables layout)
+    uint32_t nsuffix;
+    FeWords sx, sy, sz, st;   // the search's start point s B, extended
+};
+
+// Where a search stands in this step: the windows done before it and the
+// lanes it runs (a survivor's offset is decoded from them on the device).
+struct SearchPos {
+    uint64_t windows;
+    uint32_t lanes;
+    uint32_t pad;
 };
 
 struct SlotBlock {
@@ -77,6 +92,8 @@ struct Counters {
     uint32_t init_count;  // slot blocks in the init list
     uint32_t surv;        // bitmap survivors written
     uint32_t hits;        // exact hits written
+    uint32_t mismatch;    // suffix survivors whose recomputed key differed
+    uint32_t pad[3];
 };
 
 struct BatchArgs {
@@ -96,6 +113,8 @@ struct BatchArgs {
     uint32_t surv_cap;
     HitRec* hits;
     uint32_t hit_cap;
+    const SearchPos* pos;  // per descriptor
+    const uint4* pow8;     // 2^j 8G, j < 64, for the suffix key recomputation
 };
 
 __global__ void __launch_bounds__(BLOCK) batch_init_kernel(const BatchArgs a) {
@@ -133,7 +152,7 @@ __global__ void __launch_bounds__(OG_LB_THREADS, OG_LB_MIN_BLOCKS) batch_search_
         if (sb.sidx == NONE) continue;
         const BatchDesc& d = a.descs[sb.sidx];
         const uint32_t slot = item * BLOCK + threadIdx.x;
-        const Sink sink{d.bitmap, d.bits, a.surv, &a.counters->surv, a.surv_cap, sb.sidx, nullptr, 0};
+        const Sink sink{d.bitmap, d.bits, a.surv, &a.counters->surv, a.surv_cap, sb.sidx, d.sbitmap, d.sbits};
         fe x = load_fe(a.lanes + 0 * a.slots + slot, a.slots);
         fe y = load_fe(a.lanes + 2 * a.slots + slot, a.slots);
         paired_rounds(x, y, words_fe(d.wx), words_fe(d.wy), words_fe(d.wt), qtab, a.half, a.rounds,
@@ -149,7 +168,27 @@ __global__ void __launch_bounds__(256) batch_exact_kernel(const BatchArgs a) {
     const uint32_t n = min(a.counters->surv, a.surv_cap);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const HitRec r = a.surv[i];
-        const uint32_t owner = exact_owner(a.descs[r.search].match, r.y[0], r.y[1]);
+        const BatchDesc& d = a.descs[r.search];
+        uint32_t owner = d.match.nbuckets ? exact_owner(d.match, r.y[0], r.y[1]) : NONE;
+        if (owner == NONE && d.sbitmap) {
+            fe y;
+#pragma unroll
+            for (int q = 0; q < 8; q++) y.v[q] = r.y[q];
+            const uint32_t slot = suffix_slot(y, d.sbits);
+            if ((__ldg(d.sbitmap + (slot >> 5)) >> (slot & 31)) & 1u) {
+                // lane l of the search at round r of this step covers window
+                // W_done + r L + l; its candidate i has scalar offset
+                // 8 (w (2 half + 1) + 1 + i)
+                const SearchPos p = a.pos[r.search];
+                const uint32_t slots = 2 * a.half + 1;
+                const uint64_t lane = a.blocks[r.lane / BLOCK].lane0 + r.lane % BLOCK;
+                const uint64_t w = p.windows + (uint64_t)(r.step / slots) * p.lanes + lane;
+                const uint64_t k = w * slots + 1 + r.step % slots;
+                const SuffixTables t{d.suffixes, d.nsuffix, a.pow8};
+                const uint32_t j = suffix_match(t, d.sx, d.sy, d.sz, d.st, k, r.y, &a.counters->mismatch);
+                if (j != NONE) owner = d.prefix_count + j;
+            }
+        }
         if (owner != NONE) {
             const uint32_t idx = atomicAdd(&a.counters->hits, 1u);
             if (idx < a.hit_cap) {
@@ -175,12 +214,16 @@ struct Search {
     uint8_t scalar[32];
     Pt start;
     FilterSet fs;
+    SuffixSet sfx;
+    bool has_prefixes = false;
+    bool has_suffixes = false;
     bool long_filters = false;
     uint32_t quota = 0;
     uint32_t sidx = NONE;
     DevBuf<uint32_t> bitmap;
     DevBuf<uint64_t> keys;
     DevBuf<uint32_t> owners;
+    DevBuf<uint32_t> sbitmap, suffixes;
     std::vector<FilterSet::DeviceBucket> buckets;
     uint64_t table_bytes = 0;
     uint64_t windows = 0;           // W_done
@@ -206,6 +249,10 @@ struct og_batch {
     size_t smem = 0;
     DevBuf<uint4> lanes, scratch, table, pow2;
     DevBuf<BatchDesc> descs;
+    DevBuf<SearchPos> pos;
+    HostBuf<SearchPos> h_pos;
+    DevBuf<uint4> pow8;
+    uint32_t suffix_searches = 0;  // admitted searches with suffixes
     DevBuf<SlotBlock> blocks;
     DevBuf<uint32_t> init_list;
     DevBuf<Counters> counters;
@@ -329,7 +376,7 @@ void rebalance(og_batch* b, std::vector<uint32_t>& init) {
 
 int enqueue_step(og_batch* b, char* err, size_t errlen) {
     CU(cudaMemsetAsync(b->counters.p, 0, offsetof(Counters, init_count), b->stream));
-    CU(cudaMemsetAsync(&b->counters.p->surv, 0, 2 * sizeof(uint32_t), b->stream));
+    CU(cudaMemsetAsync(&b->counters.p->surv, 0, 3 * sizeof(uint32_t), b->stream));  // surv, hits, mismatch
     batch_init_kernel<<<b->nblocks, BLOCK, 0, b->stream>>>(b->args);
     CU(cudaGetLastError());
     batch_search_kernel<<<b->grid, BLOCK, b->smem, b->stream>>>(b->args);
@@ -405,6 +452,12 @@ int og_batch_new(int ordinal, const og_batch_config* cfgp, og_batch** out, char*
     CU(b->descs.alloc(cfg.max_searches));
     CU(b->h_descs.alloc(cfg.max_searches));
     std::memset(b->h_descs.p, 0, cfg.max_searches * sizeof(BatchDesc));
+    CU(b->pos.alloc(cfg.max_searches));
+    CU(b->h_pos.alloc(cfg.max_searches));
+    std::memset(b->h_pos.p, 0, cfg.max_searches * sizeof(SearchPos));
+    std::vector<uint4> p8 = pow2_table(base_mult_u64(8), 64);
+    CU(b->pow8.alloc(p8.size()));
+    CU(cudaMemcpyAsync(b->pow8.p, p8.data(), p8.size() * sizeof(uint4), cudaMemcpyHostToDevice, b->stream));
     CU(b->blocks.alloc(b->nblocks));
     CU(b->h_blocks.alloc(b->nblocks));
     CU(b->init_list.alloc(b->nblocks));
@@ -443,6 +496,8 @@ int og_batch_new(int ordinal, const og_batch_config* cfgp, og_batch** out, char*
     a.surv_cap = (uint32_t)surv_cap;
     a.hits = b->hits.p;
     a.hit_cap = cfg.max_hits;
+    a.pos = b->pos.p;
+    a.pow8 = b->pow8.p;
 
     if (cfg.graph != 2) {
         CU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
@@ -474,46 +529,60 @@ int og_batch_admit(og_batch* b, uint64_t search_id, const uint8_t seed[32], cons
     std::memcpy(s->seed, seed, 32);
     secret_scalar(seed, s->scalar);
     s->start = base_mult(s->scalar);
-    // filters
+    // filters: literal prefixes and suffixes
     std::vector<PrefixFilter> fs;
-    const char* p = filters;
-    size_t line = 0;
-    while (*p) {
-        const char* e = std::strchr(p, '\n');
-        std::string text = e ? std::string(p, (size_t)(e - p)) : std::string(p);
-        line++;
-        if (text.find_first_not_of(" \t\r") != std::string::npos) {
-            PrefixFilter f;
-            std::string why;
-            if (!parse_prefix(text, f, why)) return fail(err, errlen, OG_E_FILTER, "line %zu: %s", line, why.c_str());
-            fs.push_back(f);
-        }
-        if (!e) break;
-        p = e + 1;
-    }
+    std::vector<SuffixPattern> sfx;
     std::string why;
-    if (!s->fs.build(std::move(fs), 0, why)) return fail(err, errlen, OG_E_FILTER, "%s", why.c_str());
-    if (s->fs.occupancy() > MAX_OCCUPANCY)
+    if (!parse_filter_lines(filters, fs, sfx, why)) return fail(err, errlen, OG_E_FILTER, "%s", why.c_str());
+    if (fs.empty() && sfx.empty()) return fail(err, errlen, OG_E_FILTER, "no filters");
+    if (!fs.empty()) {
+        if (!s->fs.build(std::move(fs), 0, why)) return fail(err, errlen, OG_E_FILTER, "%s", why.c_str());
+        s->has_prefixes = true;
+    }
+    if (!sfx.empty()) {
+        if (!s->sfx.build(std::move(sfx), 0, why)) return fail(err, errlen, OG_E_FILTER, "%s", why.c_str());
+        s->has_suffixes = true;
+    }
+    const double occupancy = s->fs.occupancy() + s->sfx.occupancy();
+    if (occupancy > MAX_OCCUPANCY)
         return fail(err, errlen, OG_E_FILTER, "the filters leave %.1f%% of the index set (at most %.0f%% in a batch)",
-                    100 * s->fs.occupancy(), 100 * MAX_OCCUPANCY);
-    for (size_t i = 0; i < s->fs.size(); i++)
-        if (s->fs.filter(i).text.size() > FilterSet::DEVICE_SYMBOLS) s->long_filters = true;
+                    100 * occupancy, 100 * MAX_OCCUPANCY);
+    if (s->has_prefixes)
+        for (size_t i = 0; i < s->fs.size(); i++)
+            if (s->fs.filter(i).text.size() > FilterSet::DEVICE_SYMBOLS) s->long_filters = true;
     std::vector<uint64_t> keys;
     std::vector<uint32_t> owners;
-    s->fs.device_tables(s->buckets, keys, owners);
+    if (s->has_prefixes) s->fs.device_tables(s->buckets, keys, owners);
     if (s->buckets.size() > MAX_BUCKETS) return fail(err, errlen, OG_E_FILTER, "more than %d filter lengths", MAX_BUCKETS);
+    std::vector<uint32_t> rows;
+    for (size_t j = 0; j < s->sfx.size(); j++) {
+        const SuffixPattern& sp = s->sfx.pattern(j);
+        std::vector<uint32_t> row(MAX_SUFFIX_SYMBOLS + 1, 0);
+        row[0] = (uint32_t)sp.sets.size();
+        for (size_t i = 0; i < sp.sets.size(); i++) row[1 + i] = sp.sets[i];
+        rows.insert(rows.end(), row.begin(), row.end());
+    }
     const size_t words32 = s->fs.words().size() * 2;
-    s->table_bytes = words32 * 4 + keys.size() * 12;
+    const size_t swords32 = s->sfx.words().size() * 2;
+    s->table_bytes = words32 * 4 + keys.size() * 12 + swords32 * 4 + rows.size() * 4;
     if (b->mem_used + s->table_bytes > b->mem_budget)
         return fail(err, errlen, OG_E_NOMEM, "its tables (%llu bytes) do not fit the remaining budget (%llu of %llu used)",
                     (unsigned long long)s->table_bytes, (unsigned long long)b->mem_used, (unsigned long long)b->mem_budget);
     CU(cudaSetDevice(b->device));
-    CU(s->bitmap.alloc(words32));
-    CU(s->keys.alloc(keys.size()));
-    CU(s->owners.alloc(owners.size()));
-    CU(cudaMemcpyAsync(s->bitmap.p, s->fs.words().data(), words32 * 4, cudaMemcpyHostToDevice, b->stream));
-    CU(cudaMemcpyAsync(s->keys.p, keys.data(), keys.size() * 8, cudaMemcpyHostToDevice, b->stream));
-    CU(cudaMemcpyAsync(s->owners.p, owners.data(), owners.size() * 4, cudaMemcpyHostToDevice, b->stream));
+    if (s->has_prefixes) {
+        CU(s->bitmap.alloc(words32));
+        CU(s->keys.alloc(keys.size()));
+        CU(s->owners.alloc(owners.size()));
+        CU(cudaMemcpyAsync(s->bitmap.p, s->fs.words().data(), words32 * 4, cudaMemcpyHostToDevice, b->stream));
+        CU(cudaMemcpyAsync(s->keys.p, keys.data(), keys.size() * 8, cudaMemcpyHostToDevice, b->stream));
+        CU(cudaMemcpyAsync(s->owners.p, owners.data(), owners.size() * 4, cudaMemcpyHostToDevice, b->stream));
+    }
+    if (s->has_suffixes) {
+        CU(s->sbitmap.alloc(swords32));
+        CU(s->suffixes.alloc(rows.size()));
+        CU(cudaMemcpyAsync(s->sbitmap.p, s->sfx.words().data(), swords32 * 4, cudaMemcpyHostToDevice, b->stream));
+        CU(cudaMemcpyAsync(s->suffixes.p, rows.data(), rows.size() * 4, cudaMemcpyHostToDevice, b->stream));
+    }
     CU(cudaStreamSynchronize(b->stream));
     s->sidx = b->free_sidx.back();
     b->free_sidx.pop_back();
@@ -522,6 +591,16 @@ int og_batch_admit(og_batch* b, uint64_t search_id, const uint8_t seed[32], cons
     d.bitmap = s->bitmap.p;
     d.bits = s->fs.bits();
     d.match = match_tables(s->buckets, s->keys.p, s->owners.p);
+    d.sbitmap = s->sbitmap.p;
+    d.sbits = s->sfx.bits();
+    d.prefix_count = s->has_prefixes ? (uint32_t)s->fs.size() : 0;
+    d.suffixes = s->suffixes.p;
+    d.nsuffix = s->has_suffixes ? (uint32_t)s->sfx.size() : 0;
+    d.sx = to_words(s->start.X);
+    d.sy = to_words(s->start.Y);
+    d.sz = to_words(s->start.Z);
+    d.st = to_words(s->start.T);
+    if (s->has_suffixes) b->suffix_searches++;
     b->mark(s->sidx);
     s->admit_order = b->admitted++;
     b->mem_used += s->table_bytes;
@@ -569,6 +648,16 @@ int og_batch_step(og_batch* b, og_batch_hit* out, size_t cap, size_t* n, char* e
         b->dirty_hi = 0;
     }
     CU(cudaMemcpyAsync(b->blocks.p, b->h_blocks.p, b->nblocks * sizeof(SlotBlock), cudaMemcpyHostToDevice, b->stream));
+    if (b->suffix_searches) {
+        // where each search stands, for the device's offset decode of its
+        // suffix survivors
+        uint32_t top = 0;
+        for (Search* s : sched) {
+            b->h_pos.p[s->sidx] = SearchPos{s->windows, (uint32_t)s->blocks.size() * BLOCK, 0};
+            top = std::max(top, s->sidx + 1);
+        }
+        CU(cudaMemcpyAsync(b->pos.p, b->h_pos.p, top * sizeof(SearchPos), cudaMemcpyHostToDevice, b->stream));
+    }
     for (size_t i = 0; i < init.size(); i++) b->h_init.p[i] = init[i];
     if (!init.empty())
         CU(cudaMemcpyAsync(b->init_list.p, b->h_init.p, init.size() * 4, cudaMemcpyHostToDevice, b->stream));
@@ -589,6 +678,9 @@ int og_batch_step(og_batch* b, og_batch_hit* out, size_t cap, size_t* n, char* e
     if (c.surv > b->args.surv_cap || c.hits > b->args.hit_cap)
         return fail(err, errlen, OG_E_OVERFLOW, "a step produced %u survivors (room %u) and %u hits (room %u)", c.surv,
                     b->args.surv_cap, c.hits, b->args.hit_cap);
+    if (c.mismatch)
+        return fail(err, errlen, OG_E_VERIFY, "%u suffix survivors' keys recomputed from their offsets differ from "
+                    "the search kernel's", c.mismatch);
     // copy the exact hits back in chunks
     std::vector<HitRec> recs(c.hits);
     const size_t chunk = b->h_hits.n;
@@ -634,7 +726,8 @@ int og_batch_step(og_batch* b, og_batch_hit* out, size_t cap, size_t* n, char* e
         std::sort(v.begin(), v.end(), [](const og_batch_hit& x, const og_batch_hit& y) { return x.offset < y.offset; });
         for (og_batch_hit& h : v) {
             if (s->hits.size() >= s->quota) break;
-            if (s->long_filters) {
+            const uint32_t np = s->has_prefixes ? (uint32_t)s->fs.size() : 0;
+            if (h.filter < np && s->long_filters) {
                 const long f = s->fs.match_key(h.packed);
                 if (f < 0) continue;
                 h.filter = (uint32_t)f;
@@ -645,9 +738,19 @@ int og_batch_step(og_batch* b, og_batch_hit* out, size_t cap, size_t* n, char* e
                 continue;
             }
             std::memcpy(h.public_key, pk, 32);
-            // filters longer than the key-only span are confirmed on the address
-            const PrefixFilter& f = s->fs.filter(h.filter);
-            if (f.needs_full_check() && address(pk).compare(0, f.text.size(), f.text) != 0) continue;
+            if (h.filter < np) {
+                // filters longer than the key-only span are confirmed on the address
+                const PrefixFilter& f = s->fs.filter(h.filter);
+                if (f.needs_full_check() && address(pk).compare(0, f.text.size(), f.text) != 0) continue;
+            } else {
+                // a suffix is confirmed on the re-derived key's address
+                uint8_t addr[35];
+                address_bytes(pk, addr);
+                if (s->sfx.match_address(addr) != (long)(h.filter - np)) {
+                    b->mismatches++;
+                    continue;
+                }
+            }
             s->hits.push_back(h);
             if (out && emitted < cap) out[emitted] = h;
             emitted++;
@@ -705,6 +808,7 @@ int og_batch_retire(og_batch* b, uint64_t search_id) {
     release_blocks(b, s);
     b->free_sidx.push_back(s.sidx);
     b->mem_used -= s.table_bytes;
+    if (s.has_suffixes) b->suffix_searches--;
     if (!s.done) b->active_changed = true;
     b->searches.erase(it);
     return OG_OK;

@@ -51,34 +51,8 @@ int og_filters_new(const char* text, uint32_t bits, og_filters** out, char* err,
     *out = nullptr;
     std::vector<PrefixFilter> fs;
     std::vector<SuffixPattern> sfx;
-    const char* p = text;
-    size_t line = 0;
-    while (*p) {
-        const char* e = std::strchr(p, '\n');
-        std::string s = e ? std::string(p, (size_t)(e - p)) : std::string(p);
-        line++;
-        size_t a = 0;
-        while (a < s.size() && (s[a] == ' ' || s[a] == '\t' || s[a] == '\r')) a++;
-        if (a < s.size()) {
-            std::string why;
-            const size_t colon = s.find(':');
-            std::string form = colon == std::string::npos ? "" : s.substr(a, colon - a);
-            while (!form.empty() && (form.back() == ' ' || form.back() == '\t')) form.pop_back();
-            for (char& c : form) c = (char)std::tolower((unsigned char)c);
-            if (form == "suffix") {
-                SuffixPattern sp;
-                if (!parse_suffix(s.substr(colon + 1), sp, why))
-                    return fail(err, errlen, OG_E_FILTER, "line %zu: %s", line, why.c_str());
-                sfx.push_back(sp);
-            } else {
-                PrefixFilter f;
-                if (!parse_prefix(s, f, why)) return fail(err, errlen, OG_E_FILTER, "line %zu: %s", line, why.c_str());
-                fs.push_back(f);
-            }
-        }
-        if (!e) break;
-        p = e + 1;
-    }
+    std::string perr;
+    if (!parse_filter_lines(text, fs, sfx, perr)) return fail(err, errlen, OG_E_FILTER, "%s", perr.c_str());
     if (fs.empty() && sfx.empty()) return fail(err, errlen, OG_E_FILTER, "no filters");
     og_filters* h = new (std::nothrow) og_filters();
     if (!h) return fail(err, errlen, OG_E_NOMEM, "host memory");

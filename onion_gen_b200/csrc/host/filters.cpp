@@ -87,6 +87,42 @@ bool parse_prefix(const std::string& raw, PrefixFilter& out, std::string& err) {
     return true;
 }
 
+bool parse_filter_lines(const char* text, std::vector<PrefixFilter>& prefixes, std::vector<SuffixPattern>& suffixes,
+                        std::string& err) {
+    const char* p = text;
+    size_t line = 0;
+    while (*p) {
+        const char* e = std::strchr(p, '\n');
+        const std::string s = e ? std::string(p, (size_t)(e - p)) : std::string(p);
+        line++;
+        const std::string t = trim(s);
+        if (!t.empty()) {
+            std::string why;
+            const size_t colon = t.find(':');
+            std::string form = colon == std::string::npos ? "" : trim(t.substr(0, colon));
+            for (char& ch : form) ch = (char)std::tolower((unsigned char)ch);
+            if (form == "suffix") {
+                SuffixPattern sp;
+                if (!parse_suffix(t.substr(colon + 1), sp, why)) {
+                    err = "line " + std::to_string(line) + ": " + why;
+                    return false;
+                }
+                suffixes.push_back(sp);
+            } else {
+                PrefixFilter f;
+                if (!parse_prefix(t, f, why)) {
+                    err = "line " + std::to_string(line) + ": " + why;
+                    return false;
+                }
+                prefixes.push_back(f);
+            }
+        }
+        if (!e) break;
+        p = e + 1;
+    }
+    return true;
+}
+
 std::vector<uint64_t> build_bitmap(const std::vector<PrefixFilter>& filters, uint32_t bits) {
     std::vector<uint64_t> words;
     if (filters.empty() || bits < 8 || bits > 32) return words;

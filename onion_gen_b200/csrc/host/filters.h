@@ -78,6 +78,12 @@ private:
     std::vector<Bucket> buckets_;
 };
 
+// Parses newline-separated filters: `suffix:` lines into `suffixes`, the
+// rest (bare, `^` or `prefix:`) into `prefixes`. Blank lines are skipped;
+// an error names its line.
+bool parse_filter_lines(const char* text, std::vector<PrefixFilter>& prefixes, std::vector<SuffixPattern>& suffixes,
+                        std::string& err);
+
 // Builds the bitmap over `filters` at `bits`; empty when more than a quarter
 // of the slots would be set.
 std::vector<uint64_t> build_bitmap(const std::vector<PrefixFilter>& filters, uint32_t bits);

@@ -2,8 +2,8 @@
 // candidate numbering; field.cuh for the arithmetic.
 #include "field.cuh"
 #include "kernels.cuh"
-#include "keccak.cuh"
 #include "search_common.cuh"
+#include "suffix_match.cuh"
 
 // Register budget of the search kernels: at most OG_LB_THREADS threads per
 // block and at least OG_LB_MIN_BLOCKS resident blocks per SM. 128 x 6 caps
@@ -100,55 +100,14 @@ __global__ void __launch_bounds__(OG_LB_THREADS, 5) chain_kernel(const ChainArgs
     store_fe(a.lanes + 6 * L + lane, L, T);
 }
 
-// The filter a suffix-bitmap survivor matches, decided on its full address,
-// or 0xffffffff. Its key is recomputed from its offset: start + k 8G over
-// the binary expansion of k, then made affine; the recomputed y must equal
-// the survivor's (a mismatch is counted, never matched).
+// The filter a suffix-bitmap survivor matches (suffix_match), with the
+// survivor's scalar offset over 8 decoded from its record.
 __device__ __noinline__ uint32_t suffix_owner(const MatchArgs& a, const HitRec& r) {
     const uint64_t w = a.window0 + (uint64_t)(r.step / a.slots) * a.lanes + r.lane;
     const uint64_t k = w * a.slots + (a.paired ? 1u : 0u) + r.step % a.slots;
-    fe X = words_fe(a.sx), Y = words_fe(a.sy), Z = words_fe(a.sz), T = words_fe(a.st);
-#pragma unroll 1
-    for (uint32_t j = 0; j < 64; j++)
-        if ((k >> j) & 1) {
-            const uint4* p = a.pow8 + (size_t)j * 6;
-            add_cached(X, Y, Z, T, load_fe(p + 0, 1), load_fe(p + 2, 1), load_fe(p + 4, 1));
-        }
-    const fe zi = fe_invert(Z);
-    const fe x = fe_canon(fe_mulv(X, zi)), y = fe_canon(fe_mulv(Y, zi));
-    bool same = true;
-#pragma unroll
-    for (int q = 0; q < 8; q++) same &= y.v[q] == r.y[q];
-    if (!same) {
-        atomicAdd(a.mismatch, 1u);
-        return 0xffffffffu;
-    }
-    uint64_t pk[4];
-#pragma unroll
-    for (int q = 0; q < 4; q++) pk[q] = (uint64_t)y.v[2 * q] | ((uint64_t)y.v[2 * q + 1] << 32);
-    pk[3] |= (uint64_t)(x.v[0] & 1u) << 63;  // the sign bit
-    const uint32_t cs = onion_checksum(pk);
-    // pk || checksum || 0x03, and its base32 symbols (five bits each, most
-    // significant first)
-    uint8_t addr[36];
-#pragma unroll
-    for (int q = 0; q < 32; q++) addr[q] = (uint8_t)(pk[q / 8] >> (8 * (q % 8)));
-    addr[32] = (uint8_t)cs;
-    addr[33] = (uint8_t)(cs >> 8);
-    addr[34] = 0x03;
-    addr[35] = 0;
-    for (uint32_t j = 0; j < a.nsuffix; j++) {
-        const uint32_t* s = a.suffixes + (size_t)j * (MAX_SUFFIX_SYMBOLS + 1);
-        const uint32_t len = s[0], start = MAX_SUFFIX_SYMBOLS - len;
-        bool ok = true;
-        for (uint32_t i = 0; i < len && ok; i++) {
-            const uint32_t bit = (start + i) * 5, byte = bit / 8;
-            const uint32_t sym = ((((uint32_t)addr[byte] << 8) | addr[byte + 1]) >> (11 - bit % 8)) & 31u;
-            ok = (s[1 + i] >> sym) & 1u;
-        }
-        if (ok) return a.prefix_count + j;
-    }
-    return 0xffffffffu;
+    const SuffixTables t{a.suffixes, a.nsuffix, a.pow8};
+    const uint32_t j = suffix_match(t, a.sx, a.sy, a.sz, a.st, k, r.y, a.mismatch);
+    return j == 0xffffffffu ? j : a.prefix_count + j;
 }
 
 // Exact match of one advance's bitmap survivors (grid-stride; the survivor

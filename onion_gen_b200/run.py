@@ -1,7 +1,8 @@
 """The device search loop of onion-gen's run driver (src/run.rs:1030-1119).
 
 ``device_search`` drives one ``gpu.Engine`` the way ``run::device_worker``
-does: advance, confirm every survivor exactly against the filter set, re-derive
+does: advance, confirm every survivor exactly against the filter set (on the
+device for suffixes, whose address needs the sign bit and checksum), re-derive
 the key of every match from its offset on the host and compare it with the
 device's bytes, and stop once ``quota`` hits are in hand. It returns the
 first ``quota`` hits in offset order: every advance covers the next contiguous
@@ -32,11 +33,17 @@ def device_search(device, seed: bytes, prefixes, quota: int, threads: int = 0, c
     (og_engine_advance_matches): only matches cross back, the same ones the
     host match finds."""
     fs = F.FilterSet.parse_all(prefixes)
-    words, bits = fs.index_words()
     start = key.start_point(seed)
-    eng = gpu.Engine(device, start, threads=threads, bitmap=words, bitmap_bits=bits, config=config)
-    if device_match:
-        eng.match_on_device(fs)
+    np_ = fs.prefix_count()
+    if np_ < len(fs):
+        # suffixes: the filter engine (both bitmaps, the device match on)
+        eng = gpu.Engine(device, start, filters=fs, config=config)
+        device_match = True
+    else:
+        words, bits = fs.index_words()
+        eng = gpu.Engine(device, start, threads=threads, bitmap=words, bitmap_bits=bits, config=config)
+        if device_match:
+            eng.match_on_device(fs)
     texts = fs.texts()
     found = []
     advances = 0
@@ -59,7 +66,10 @@ def device_search(device, seed: bytes, prefixes, quota: int, threads: int = 0, c
             for j in idx[np.argsort(offsets[idx], kind="stable")]:
                 off, b, f = int(offsets[j]), bytes(packed[j]), int(matched[j])
                 pk, _ = key.check_hit(seed, off, b)
-                if len(texts[f]) > 49 and not key.address(pk).startswith(texts[f]):
+                if f >= np_:
+                    if fs.match_address(pk) != f:  # a suffix: confirmed on the address
+                        continue
+                elif len(texts[f]) > 49 and not key.address(pk).startswith(texts[f]):
                     continue
                 found.append(Found(off, b, pk, f))
                 if len(found) == quota:

@@ -163,3 +163,39 @@ def test_tuner_records_a_shape_that_finds_the_same_hits(device, mixed, tmp_path,
     out, _ = mixed
     tuned, _ = run_batch(device, SEARCHES, half=0, slots=0)
     assert tuned == out
+
+
+SUFFIX_SEARCHES = [
+    (201, workloads.suffix_filters(6, 8), 1),
+    (202, workloads.suffix_filters(12, 8)[6:] + ["abc"], 2),
+    (203, ["xy", "suffix:" + "q" * 6 + "id"], 3),
+]
+
+
+def test_suffix_searches_in_a_batch_agree_with_the_single_engine(device):
+    """Suffix searches (alone and mixed with prefixes) in the batch find the
+    same first hits as the single filter engine; every suffix hit's address
+    really ends in its suffix."""
+    b = B.Batch(device, half=256)
+    for sid, filters, quota in SUFFIX_SEARCHES:
+        b.admit(sid, workloads.seed(sid), filters, quota)
+    steps = 0
+    while b.running():
+        b.step()
+        steps += 1
+        assert steps < 400
+    from onion_gen_b200 import filter as F
+    from onion_gen_b200 import key
+
+    for sid, filters, quota in SUFFIX_SEARCHES:
+        got = b.results(sid)
+        assert len(got) == quota
+        cfg = N.EngineConfig(0, 256, 0, 1, 128, 0, 0)
+        found, _, _ = run.device_search(device, workloads.seed(sid), filters, quota, config=cfg, max_advances=200)
+        assert [(h.offset, h.packed) for h in found] == [key_of(h) for h in got], sid
+        texts = F.FilterSet.parse_all(filters).texts()
+        for h in got:
+            t = texts[h.filter]
+            addr = key.address(h.public_key)
+            assert addr.endswith(t[7:]) if t.startswith("suffix:") else addr.startswith(t)
+    b.close()

@@ -221,9 +221,12 @@ int og_batch_tune(int ordinal, uint32_t searches, float max_step_ms, og_batch_co
                   char* err, size_t errlen);
 /* The shape a batch runs (defaults filled in). */
 void og_batch_shape(const og_batch* b, og_batch_config* cfg);
-/* Admits a search: `filters` newline-separated literal prefixes. Fails with
- * OG_E_NOMEM when its tables do not fit the memory budget (nothing is
- * changed), OG_E_CAPACITY when max_searches are admitted. */
+/* Admits a search: `filters` newline-separated, literal prefixes and
+ * `suffix:` lines as og_filters_new takes them (a suffix hit's key, sign
+ * bit and checksum are recomputed on the device). Fails with OG_E_NOMEM
+ * when its tables do not fit the memory budget (nothing is changed),
+ * OG_E_CAPACITY when max_searches are admitted, OG_E_FILTER when its
+ * bitmaps would let more than 2% of the candidates through. */
 int og_batch_admit(og_batch* b, uint64_t search_id, const uint8_t seed[32], const char* filters, uint32_t quota,
                    char* err, size_t errlen);
 /* One step: every admitted, unfinished search advances `rounds` rounds.
@@ -287,7 +290,9 @@ typedef struct og_serve_stats {
 } og_serve_stats;
 
 int og_serve_new(int ordinal, const og_serve_config* cfg, og_serve** out, char* err, size_t errlen);
-/* Queues a request (thread-safe); the arrival time is taken here. */
+/* Queues a request (thread-safe); the arrival time is taken here. `filters`
+ * as og_batch_admit takes them; a request the batch refuses completes with
+ * that status. */
 int og_serve_submit(og_serve* s, uint64_t request_id, const uint8_t seed[32], const char* filters, uint32_t quota,
                     char* err, size_t errlen);
 /* Requests completed since the last poll, in completion order. */

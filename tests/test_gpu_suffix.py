@@ -112,3 +112,14 @@ def test_an_engine_without_suffix_bitmap_refuses_a_suffix_set(device):
     with pytest.raises(N.OgError) as e:
         eng.match_on_device(sfx)
     assert e.value.status == "OG_E_ARG"
+
+
+def test_run_driver_with_a_prefix_and_a_suffix(device):
+    """The package's front door on a mixed set, as a user calls it."""
+    from onion_gen_b200 import run
+
+    hits, examined, advances = run.device_search(device, workloads.seed(0), ["abcd", "suffix:zzzzzzzqd"], quota=2)
+    assert len(hits) == 2 and advances >= 1 and examined > 0
+    for h in hits:
+        addr = key.address(h.public_key)
+        assert addr.startswith("abcd") or addr.endswith("zzzzzzzqd")

@@ -385,10 +385,13 @@ int og_check_hit(const uint8_t seed[32], uint64_t offset, const uint8_t packed[3
 
 typedef struct og_filters og_filters;
 
-/* Newline-separated filters (Pattern::parse, src/filter.rs:298-350): literal
- * prefixes (bare, `^` or `prefix:`) and `suffix:` forms whose symbols may
- * be `?` or `[...]` classes (parse_symbols, :495-560), checked against the
- * v3 address tail (:566-600). `bits` is the prefix index width, 0 to choose
+/* Newline-separated filters (Pattern::parse, src/filter.rs:298-350):
+ * prefixes (bare, `^` or `prefix:`) and `suffix:` forms, whose symbols may
+ * be `?` or `[...]` classes (parse_symbols, :495-560); suffixes are checked
+ * against the v3 address tail (:566-600). A prefix with wildcards or classes
+ * fills every slot it allows in the prefix bitmap (pattern_slots,
+ * :2480-2530; more than 4096 slots cannot be indexed: OG_E_FILTER) and is
+ * matched after the literal prefixes, in order. `bits` is the prefix index width, 0 to choose
  * it; the suffix index width is always chosen (:1420-1440). A suffix that
  * reaches too little of the key for a suffix bitmap is OG_E_FILTER. */
 int og_filters_new(const char* text, uint32_t bits, og_filters** out, char* err, size_t errlen);

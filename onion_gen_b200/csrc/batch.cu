@@ -48,7 +48,8 @@ namespace og {
 const std::vector<uint4>& pair_table(uint32_t half);           // engine.cu
 std::vector<uint4> pow2_table(const Pt& stride, uint32_t nbits);  // engine.cu
 MatchTables match_tables(const std::vector<FilterSet::DeviceBucket>& buckets, const uint64_t* keys,
-                         const uint32_t* owners);                  // engine.cu
+                         const uint32_t* owners, const uint32_t* patterns,
+                         uint32_t npatterns);                      // engine.cu
 
 namespace {
 
@@ -169,7 +170,7 @@ __global__ void __launch_bounds__(256) batch_exact_kernel(const BatchArgs a) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const HitRec r = a.surv[i];
         const BatchDesc& d = a.descs[r.search];
-        uint32_t owner = d.match.nbuckets ? exact_owner(d.match, r.y[0], r.y[1]) : NONE;
+        uint32_t owner = (d.match.nbuckets || d.match.npatterns) ? exact_owner(d.match, r.y) : NONE;
         if (owner == NONE && d.sbitmap) {
             fe y;
 #pragma unroll
@@ -223,7 +224,7 @@ struct Search {
     DevBuf<uint32_t> bitmap;
     DevBuf<uint64_t> keys;
     DevBuf<uint32_t> owners;
-    DevBuf<uint32_t> sbitmap, suffixes;
+    DevBuf<uint32_t> sbitmap, suffixes, patterns;
     std::vector<FilterSet::DeviceBucket> buckets;
     uint64_t table_bytes = 0;
     uint64_t windows = 0;           // W_done
@@ -549,10 +550,14 @@ int og_batch_admit(og_batch* b, uint64_t search_id, const uint8_t seed[32], cons
                     100 * occupancy, 100 * MAX_OCCUPANCY);
     if (s->has_prefixes)
         for (size_t i = 0; i < s->fs.size(); i++)
-            if (s->fs.filter(i).text.size() > FilterSet::DEVICE_SYMBOLS) s->long_filters = true;
+            if (!s->fs.filter(i).is_pattern() && s->fs.filter(i).text.size() > FilterSet::DEVICE_SYMBOLS)
+            s->long_filters = true;
     std::vector<uint64_t> keys;
-    std::vector<uint32_t> owners;
-    if (s->has_prefixes) s->fs.device_tables(s->buckets, keys, owners);
+    std::vector<uint32_t> owners, pats;
+    if (s->has_prefixes) {
+        s->fs.device_tables(s->buckets, keys, owners);
+        s->fs.device_patterns(pats);
+    }
     if (s->buckets.size() > MAX_BUCKETS) return fail(err, errlen, OG_E_FILTER, "more than %d filter lengths", MAX_BUCKETS);
     std::vector<uint32_t> rows;
     for (size_t j = 0; j < s->sfx.size(); j++) {
@@ -564,7 +569,7 @@ int og_batch_admit(og_batch* b, uint64_t search_id, const uint8_t seed[32], cons
     }
     const size_t words32 = s->fs.words().size() * 2;
     const size_t swords32 = s->sfx.words().size() * 2;
-    s->table_bytes = words32 * 4 + keys.size() * 12 + swords32 * 4 + rows.size() * 4;
+    s->table_bytes = words32 * 4 + keys.size() * 12 + pats.size() * 4 + swords32 * 4 + rows.size() * 4;
     if (b->mem_used + s->table_bytes > b->mem_budget)
         return fail(err, errlen, OG_E_NOMEM, "its tables (%llu bytes) do not fit the remaining budget (%llu of %llu used)",
                     (unsigned long long)s->table_bytes, (unsigned long long)b->mem_used, (unsigned long long)b->mem_budget);
@@ -576,6 +581,10 @@ int og_batch_admit(og_batch* b, uint64_t search_id, const uint8_t seed[32], cons
         CU(cudaMemcpyAsync(s->bitmap.p, s->fs.words().data(), words32 * 4, cudaMemcpyHostToDevice, b->stream));
         CU(cudaMemcpyAsync(s->keys.p, keys.data(), keys.size() * 8, cudaMemcpyHostToDevice, b->stream));
         CU(cudaMemcpyAsync(s->owners.p, owners.data(), owners.size() * 4, cudaMemcpyHostToDevice, b->stream));
+        if (!pats.empty()) {
+            CU(s->patterns.alloc(pats.size()));
+            CU(cudaMemcpyAsync(s->patterns.p, pats.data(), pats.size() * 4, cudaMemcpyHostToDevice, b->stream));
+        }
     }
     if (s->has_suffixes) {
         CU(s->sbitmap.alloc(swords32));
@@ -590,7 +599,8 @@ int og_batch_admit(og_batch* b, uint64_t search_id, const uint8_t seed[32], cons
     std::memset(&d, 0, sizeof d);
     d.bitmap = s->bitmap.p;
     d.bits = s->fs.bits();
-    d.match = match_tables(s->buckets, s->keys.p, s->owners.p);
+    d.match = match_tables(s->buckets, s->keys.p, s->owners.p, s->patterns.p,
+                           (uint32_t)(pats.size() / FilterSet::PATTERN_ROW));
     d.sbitmap = s->sbitmap.p;
     d.sbits = s->sfx.bits();
     d.prefix_count = s->has_prefixes ? (uint32_t)s->fs.size() : 0;
@@ -741,7 +751,7 @@ int og_batch_step(og_batch* b, og_batch_hit* out, size_t cap, size_t* n, char* e
             if (h.filter < np) {
                 // filters longer than the key-only span are confirmed on the address
                 const PrefixFilter& f = s->fs.filter(h.filter);
-                if (f.needs_full_check() && address(pk).compare(0, f.text.size(), f.text) != 0) continue;
+                if (f.needs_full_check() && !f.matches_address(address(pk))) continue;
             } else {
                 // a suffix is confirmed on the re-derived key's address
                 uint8_t addr[35];

@@ -101,11 +101,15 @@ uint32_t bits_for(uint64_t v) {
     return b;
 }
 
+static_assert(FilterSet::PATTERN_ROW == PATTERN_WORDS, "pattern rows: host and device layouts agree");
+
 MatchTables match_tables(const std::vector<FilterSet::DeviceBucket>& buckets, const uint64_t* keys,
-                         const uint32_t* owners) {
+                         const uint32_t* owners, const uint32_t* patterns, uint32_t npatterns) {
     MatchTables t{};
     t.keys = keys;
     t.owners = owners;
+    t.patterns = patterns;
+    t.npatterns = npatterns;
     t.nbuckets = (uint32_t)std::min<size_t>(buckets.size(), MAX_MATCH_BUCKETS);
     for (uint32_t i = 0; i < t.nbuckets; i++) {
         t.bucket_bits[i] = buckets[i].bits;
@@ -160,7 +164,7 @@ struct og_engine {
     uint32_t prefix_count = 0;
     og::FilterSet fs;
     DevBuf<uint64_t> mkeys;
-    DevBuf<uint32_t> mowners, mcount;
+    DevBuf<uint32_t> mowners, mcount, mpatterns;
     DevBuf<HitRec> matches;
     HostBuf<HitRec> h_matches;
     HostBuf<uint32_t> h_mcount;
@@ -408,8 +412,11 @@ double time_advance(og_engine* e, std::vector<og_survivor>& buf) {
 int enable_matching(og_engine* e, const og_filters* f, char* err, size_t errlen) {
     std::vector<FilterSet::DeviceBucket> buckets;
     std::vector<uint64_t> keys;
-    std::vector<uint32_t> owners;
-    if (f->has_prefixes) f->set.device_tables(buckets, keys, owners);
+    std::vector<uint32_t> owners, pats;
+    if (f->has_prefixes) {
+        f->set.device_tables(buckets, keys, owners);
+        f->set.device_patterns(pats);
+    }
     if (buckets.size() > (size_t)MAX_MATCH_BUCKETS)
         return fail(err, errlen, OG_E_FILTER, "more than %d filter lengths", MAX_MATCH_BUCKETS);
     std::vector<uint32_t> sfx;
@@ -431,6 +438,10 @@ int enable_matching(og_engine* e, const og_filters* f, char* err, size_t errlen)
         CU(cudaMemcpyAsync(e->mkeys.p, keys.data(), keys.size() * 8, cudaMemcpyHostToDevice, e->stream));
         CU(cudaMemcpyAsync(e->mowners.p, owners.data(), owners.size() * 4, cudaMemcpyHostToDevice, e->stream));
     }
+    if (!pats.empty()) {
+        CU(e->mpatterns.alloc(pats.size()));
+        CU(cudaMemcpyAsync(e->mpatterns.p, pats.data(), pats.size() * 4, cudaMemcpyHostToDevice, e->stream));
+    }
     std::vector<uint4> pw;
     if (!sfx.empty()) {
         CU(e->suffixes.alloc(sfx.size()));
@@ -450,14 +461,16 @@ int enable_matching(og_engine* e, const og_filters* f, char* err, size_t errlen)
     e->long_filters = false;
     if (f->has_prefixes)
         for (size_t i = 0; i < e->fs.size(); i++)
-            if (e->fs.filter(i).text.size() > FilterSet::DEVICE_SYMBOLS) e->long_filters = true;
+            if (!e->fs.filter(i).is_pattern() && e->fs.filter(i).text.size() > FilterSet::DEVICE_SYMBOLS)
+                e->long_filters = true;
     e->prefix_count = f->has_prefixes ? (uint32_t)f->set.size() : 0;
     MatchArgs& m = e->ma;
     m = MatchArgs{};
     m.surv = e->hits.p;
     m.surv_count = e->counter.p;
     m.surv_cap = (uint32_t)std::min<size_t>(e->cap, 0xffffffffu);
-    m.t = match_tables(buckets, e->mkeys.p, e->mowners.p);
+    m.t = match_tables(buckets, e->mkeys.p, e->mowners.p, e->mpatterns.p,
+                       (uint32_t)(pats.size() / FilterSet::PATTERN_ROW));
     m.sbitmap = sfx.empty() ? nullptr : e->sbitmap.p;
     m.sbits = e->sbits;
     m.suffixes = e->suffixes.p;

@@ -110,7 +110,7 @@ long og_filters_match_address(const og_filters* f, const uint8_t pk[32]) {
         const long m = f->set.match_key(pk);
         if (m >= 0) {
             const PrefixFilter& pf = f->set.filter((size_t)m);
-            if (!pf.needs_full_check() || address(pk).compare(0, pf.text.size(), pf.text) == 0) return m;
+            if (!pf.needs_full_check() || pf.matches_address(address(pk))) return m;
         }
     }
     if (f->has_suffixes) {

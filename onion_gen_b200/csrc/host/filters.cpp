@@ -28,9 +28,50 @@ size_t slot_of(const uint8_t packed[32], uint32_t bits) { return (size_t)(head64
 
 }  // namespace
 
+// Every slot of a `bits`-wide prefix index a pattern can occupy: the values its
+// sets allow over the first bits / 5 symbols and the top bits % 5 bits of the
+// next; false past 4096 slots (BitmapIndex::pattern_slots, src/filter.rs:2480-2530).
+bool pattern_slots(const PrefixFilter& f, uint32_t bits, std::vector<uint32_t>& out) {
+    const uint32_t full = bits / 5, rem = bits % 5;
+    std::vector<uint32_t> values{0};
+    for (uint32_t k = 0; k < full + (rem ? 1 : 0); k++) {
+        const uint32_t set = k < f.sets.size() ? f.sets[k] : 0xffffffffu;
+        uint32_t parts = 0;
+        for (uint32_t v = 0; v < 32; v++)
+            if ((set >> v) & 1) parts |= 1u << (k < full ? v : v >> (5 - rem));
+        const size_t np = (size_t)__builtin_popcount(parts);
+        if (values.size() * np > 4096) return false;
+        const uint32_t shift = k < full ? bits - 5 * (k + 1) : 0;
+        std::vector<uint32_t> next;
+        next.reserve(values.size() * np);
+        for (uint32_t base : values)
+            for (uint32_t part = 0; part < 32; part++)
+                if ((parts >> part) & 1) next.push_back(base | (part << shift));
+        values.swap(next);
+    }
+    out.swap(values);
+    return true;
+}
+
 bool PrefixFilter::matches_key(const uint8_t packed[32]) const {
+    if (is_pattern()) {
+        const size_t m = std::min(sets.size(), KEY_ONLY_SYMBOLS);
+        for (size_t i = 0; i < m; i++)
+            if (!((sets[i] >> symbol_at(packed, 32, i)) & 1)) return false;
+        return true;
+    }
     const size_t last = nbytes - 1;
     return std::memcmp(packed, bytes, last) == 0 && (packed[last] & mask) == bytes[last];
+}
+
+bool PrefixFilter::matches_address(const std::string& address) const {
+    if (!is_pattern()) return address.compare(0, text.size(), text) == 0;
+    if (address.size() < sets.size()) return false;
+    for (size_t i = 0; i < sets.size(); i++) {
+        const int v = base32_value(address[i]);
+        if (v < 0 || !((sets[i] >> v) & 1)) return false;
+    }
+    return true;
 }
 
 bool parse_prefix(const std::string& raw, PrefixFilter& out, std::string& err) {
@@ -53,6 +94,26 @@ bool parse_prefix(const std::string& raw, PrefixFilter& out, std::string& err) {
         err = "the filter is empty";
         return false;
     }
+    if (s.find_first_of("?[]") != std::string::npos) {
+        // a pattern: wildcards or classes (Pattern::parse, src/filter.rs:298-350)
+        std::vector<uint32_t> sets;
+        if (!parse_symbol_sets(s, sets, err)) return false;
+        if (sets.size() > ADDRESS_SYMBOLS) {
+            err = "a filter of " + std::to_string(sets.size()) + " symbols is longer than an address (56)";
+            return false;
+        }
+        if (std::all_of(sets.begin(), sets.end(), [](uint32_t x) { return x == 0xffffffffu; })) {
+            err = "the filter fixes no symbol";
+            return false;
+        }
+        out.sets = sets;
+        out.text = render_sets(sets);
+        out.nbytes = 0;
+        out.mask = 0;
+        std::memset(out.bytes, 0, sizeof out.bytes);
+        return true;
+    }
+    out.sets.clear();
     if (s.size() > ADDRESS_SYMBOLS) {
         err = "a filter of " + std::to_string(s.size()) + " symbols is longer than an address (56)";
         return false;
@@ -128,6 +189,12 @@ std::vector<uint64_t> build_bitmap(const std::vector<PrefixFilter>& filters, uin
     if (filters.empty() || bits < 8 || bits > 32) return words;
     words.assign((size_t)(((1ULL << bits) + 63) / 64), 0);
     for (const PrefixFilter& f : filters) {
+        if (f.is_pattern()) {
+            std::vector<uint32_t> slots;
+            if (!pattern_slots(f, bits, slots)) return {};
+            for (uint32_t v : slots) words[v >> 6] |= 1ULL << (v & 63);
+            continue;
+        }
         const size_t sym = std::min(f.text.size(), KEY_ONLY_SYMBOLS);
         const uint32_t pbits = (uint32_t)(sym * 5);
         uint8_t probe[32] = {0};
@@ -164,8 +231,21 @@ bool FilterSet::build(std::vector<PrefixFilter> filters, uint32_t bits, std::str
     std::sort(filters.begin(), filters.end(),
               [](const PrefixFilter& a, const PrefixFilter& b) { return a.text < b.text; });
     filters_.clear();
+    long last_literal = -1;
     for (PrefixFilter& f : filters) {
-        if (!filters_.empty() && f.text.compare(0, filters_.back().text.size(), filters_.back().text) == 0) continue;
+        if (f.is_pattern()) {
+            // patterns: exact duplicates only
+            bool dup = false;
+            for (const PrefixFilter& g : filters_) dup |= g.is_pattern() && g.text == f.text;
+            if (!dup) filters_.push_back(f);
+            continue;
+        }
+        // a literal prefix absorbs the literals it starts (src/filter.rs:1326-1339)
+        if (last_literal >= 0) {
+            const std::string& prev = filters_[(size_t)last_literal].text;
+            if (f.text.compare(0, prev.size(), prev) == 0) continue;
+        }
+        last_literal = (long)filters_.size();
         filters_.push_back(f);
     }
     if (filters_.empty()) {
@@ -199,7 +279,12 @@ bool FilterSet::build(std::vector<PrefixFilter> filters, uint32_t bits, std::str
     }
     // length buckets for the exact match
     buckets_.clear();
+    patterns_.clear();
     for (size_t i = 0; i < filters_.size(); i++) {
+        if (filters_[i].is_pattern()) {
+            patterns_.push_back((uint32_t)i);
+            continue;
+        }
         const size_t sym = std::min(filters_[i].text.size(), KEY_ONLY_SYMBOLS);
         auto it = std::find_if(buckets_.begin(), buckets_.end(), [&](const Bucket& b) { return b.symbols == sym; });
         if (it == buckets_.end()) {
@@ -250,6 +335,8 @@ long FilterSet::match_key(const uint8_t packed[32]) const {
             if (filters_[owner].matches_key(packed)) return (long)owner;
         }
     }
+    for (uint32_t i : patterns_)
+        if (filters_[i].matches_key(packed)) return (long)i;
     return -1;
 }
 
@@ -260,6 +347,7 @@ void FilterSet::device_tables(std::vector<DeviceBucket>& buckets, std::vector<ui
     owners.clear();
     std::vector<std::vector<std::pair<uint64_t, uint32_t>>> by_len(DEVICE_SYMBOLS + 1);
     for (size_t i = 0; i < filters_.size(); i++) {
+        if (filters_[i].is_pattern()) continue;
         const size_t sym = std::min(filters_[i].text.size(), DEVICE_SYMBOLS);
         const uint32_t hb = (uint32_t)(sym * 5);
         uint8_t padded[32] = {0};
@@ -278,9 +366,30 @@ void FilterSet::device_tables(std::vector<DeviceBucket>& buckets, std::vector<ui
     }
 }
 
+void FilterSet::device_patterns(std::vector<uint32_t>& rows) const {
+    rows.clear();
+    for (uint32_t i : patterns_) {
+        const PrefixFilter& f = filters_[i];
+        std::vector<uint32_t> row(PATTERN_ROW, 0xffffffffu);
+        row[0] = i;
+        row[1] = (uint32_t)std::min(f.sets.size(), KEY_ONLY_SYMBOLS);
+        for (size_t k = 0; k < row[1]; k++) row[2 + k] = f.sets[k];
+        rows.insert(rows.end(), row.begin(), row.end());
+    }
+}
+
 double FilterSet::match_probability() const {
     double p = 0;
-    for (const PrefixFilter& f : filters_) p += std::pow(32.0, -(double)std::min(f.text.size(), KEY_ONLY_SYMBOLS));
+    for (const PrefixFilter& f : filters_) {
+        if (f.is_pattern()) {
+            double q = 1;
+            for (size_t i = 0; i < std::min(f.sets.size(), KEY_ONLY_SYMBOLS); i++)
+                q *= __builtin_popcount(f.sets[i]) / 32.0;
+            p += q;
+        } else {
+            p += std::pow(32.0, -(double)std::min(f.text.size(), KEY_ONLY_SYMBOLS));
+        }
+    }
     return std::min(p, 1.0);
 }
 

@@ -22,13 +22,20 @@ constexpr size_t KEY_ONLY_SYMBOLS = 49;
 constexpr size_t ADDRESS_SYMBOLS = 56;
 
 struct PrefixFilter {
-    std::string text;  // canonical: lowercase symbols
-    uint8_t bytes[32];
+    std::string text;  // canonical: lowercase symbols; a pattern's `?` and classes rendered
+    uint8_t bytes[32];  // a literal's first min(len, 49) symbols decoded
     size_t nbytes;
     uint8_t mask;
+    std::vector<uint32_t> sets;  // a pattern's symbol set per position; empty for a literal
+    bool is_pattern() const { return !sets.empty(); }
+    size_t symbols() const { return is_pattern() ? sets.size() : text.size(); }
     // filters longer than the key-only span need the full address checked
-    bool needs_full_check() const { return text.size() > KEY_ONLY_SYMBOLS; }
+    bool needs_full_check() const { return symbols() > KEY_ONLY_SYMBOLS; }
+    // the key-only part: a masked byte compare, or a pattern's sets over the
+    // first min(len, 49) symbols
     bool matches_key(const uint8_t packed[32]) const;
+    // the full check on an address text of 56 symbols
+    bool matches_address(const std::string& address) const;
 };
 
 // Parses one filter; returns false and an explanation on error.
@@ -64,6 +71,11 @@ public:
     };
     void device_tables(std::vector<DeviceBucket>& buckets, std::vector<uint64_t>& keys,
                        std::vector<uint32_t>& owners) const;
+    // The patterns in the form the device walks after the buckets, in index
+    // order: per pattern PATTERN_ROW words, its filter index, the number of
+    // key-only symbols it fixes (at most 49) and one set per position.
+    static constexpr size_t PATTERN_ROW = 2 + KEY_ONLY_SYMBOLS;
+    void device_patterns(std::vector<uint32_t>& rows) const;
 
 private:
     struct Bucket {
@@ -76,7 +88,10 @@ private:
     std::vector<uint64_t> words_;
     uint32_t bits_ = 0;
     std::vector<Bucket> buckets_;
+    std::vector<uint32_t> patterns_;  // indices of the patterns, in order
 };
+
+bool pattern_slots(const PrefixFilter& f, uint32_t bits, std::vector<uint32_t>& out);
 
 // Parses newline-separated filters: `suffix:` lines into `suffixes`, the
 // rest (bare, `^` or `prefix:`) into `prefixes`. Blank lines are skipped;

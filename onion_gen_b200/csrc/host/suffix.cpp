@@ -17,22 +17,7 @@ constexpr size_t SLOT_BUDGET = 4096;  // past this many slots one suffix fills t
 // bit, which is worth 2 within symbol 49 (bits 245..249, the sign at 248).
 uint32_t either_sign(uint32_t set) { return set | ((set & 0x33333333u) << 2) | ((set & 0xccccccccu) >> 2); }
 
-std::string render(const std::vector<uint32_t>& sets) {
-    std::string s = "suffix:";
-    for (uint32_t set : sets) {
-        if (set == ALL) {
-            s.push_back('?');
-        } else if (__builtin_popcount(set) == 1) {
-            s.push_back(BASE32_ALPHABET[__builtin_ctz(set)]);
-        } else {
-            s.push_back('[');
-            for (int v = 0; v < 32; v++)
-                if ((set >> v) & 1) s.push_back(BASE32_ALPHABET[v]);
-            s.push_back(']');
-        }
-    }
-    return s;
-}
+std::string render(const std::vector<uint32_t>& sets) { return "suffix:" + render_sets(sets); }
 
 std::string where(size_t i) { return " at position " + std::to_string(i); }
 
@@ -62,12 +47,8 @@ bool SuffixPattern::key_prefilter(const uint8_t packed[32]) const {
     return true;
 }
 
-bool parse_suffix(const std::string& raw, SuffixPattern& out, std::string& err) {
-    size_t a = 0, b = raw.size();
-    while (a < b && (raw[a] == ' ' || raw[a] == '\t' || raw[a] == '\r')) a++;
-    while (b > a && (raw[b - 1] == ' ' || raw[b - 1] == '\t' || raw[b - 1] == '\r')) b--;
-    const std::string body = raw.substr(a, b - a);
-    std::vector<uint32_t> sets;
+bool parse_symbol_sets(const std::string& body, std::vector<uint32_t>& sets, std::string& err) {
+    sets.clear();
     for (size_t i = 0; i < body.size();) {
         const char c = body[i];
         if (c == '?') {
@@ -122,6 +103,33 @@ bool parse_suffix(const std::string& raw, SuffixPattern& out, std::string& err) 
             i++;
         }
     }
+    return true;
+}
+
+std::string render_sets(const std::vector<uint32_t>& sets) {
+    std::string s;
+    for (uint32_t set : sets) {
+        if (set == ALL) {
+            s.push_back('?');
+        } else if (__builtin_popcount(set) == 1) {
+            s.push_back(BASE32_ALPHABET[__builtin_ctz(set)]);
+        } else {
+            s.push_back('[');
+            for (int v = 0; v < 32; v++)
+                if ((set >> v) & 1) s.push_back(BASE32_ALPHABET[v]);
+            s.push_back(']');
+        }
+    }
+    return s;
+}
+
+bool parse_suffix(const std::string& raw, SuffixPattern& out, std::string& err) {
+    size_t a = 0, b = raw.size();
+    while (a < b && (raw[a] == ' ' || raw[a] == '\t' || raw[a] == '\r')) a++;
+    while (b > a && (raw[b - 1] == ' ' || raw[b - 1] == '\t' || raw[b - 1] == '\r')) b--;
+    const std::string body = raw.substr(a, b - a);
+    std::vector<uint32_t> sets;
+    if (!parse_symbol_sets(body, sets, err)) return false;
     if (sets.empty()) {
         err = "the filter is empty";
         return false;

@@ -39,6 +39,12 @@ struct SuffixPattern {
     bool key_prefilter(const uint8_t packed[32]) const;
 };
 
+// A filter body as one symbol set per position: literal symbols, `?` (any)
+// and `[...]` classes with `a-e` ranges (parse_symbols, src/filter.rs:495-560).
+bool parse_symbol_sets(const std::string& body, std::vector<uint32_t>& sets, std::string& err);
+// The canonical text of symbol sets: a symbol, `?`, or the class's members.
+std::string render_sets(const std::vector<uint32_t>& sets);
+
 // Parses the body of a `suffix:` filter (without the form name).
 bool parse_suffix(const std::string& body, SuffixPattern& out, std::string& err);
 

@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(128) match_kernel(const MatchArgs a) {
     const uint32_t n = min(*a.surv_count, a.surv_cap);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const HitRec r = a.surv[i];
-        uint32_t owner = a.t.nbuckets ? exact_owner(a.t, r.y[0], r.y[1]) : 0xffffffffu;
+        uint32_t owner = (a.t.nbuckets || a.t.npatterns) ? exact_owner(a.t, r.y) : 0xffffffffu;
         if (owner == 0xffffffffu && a.sbitmap) {
             fe y;
 #pragma unroll

@@ -106,7 +106,13 @@ struct MatchTables {
     uint32_t bucket_bits[MAX_MATCH_BUCKETS];
     uint32_t bucket_off[MAX_MATCH_BUCKETS];
     uint32_t bucket_len[MAX_MATCH_BUCKETS];
+    // prefixes with wildcards or classes, walked after the buckets: per
+    // pattern PATTERN_WORDS words, its filter index, the key-only symbols it
+    // fixes (at most 49) and one symbol set per position
+    const uint32_t* patterns;
+    uint32_t npatterns;
 };
+constexpr uint32_t PATTERN_WORDS = 2 + 49;
 
 // The single engine's exact match over one advance's bitmap survivors:
 // matching records are copied to `out` with `pad` = the filter's index.

@@ -104,12 +104,21 @@ __device__ __forceinline__ void test_emit(const Sink& k, const fe& yraw, uint32_
     }
 }
 
-// The filter a canonical key matches exactly on its first 12 symbols at
-// most, or 0xffffffff: per length bucket, a binary search of the sorted
-// masked heads. No kept filter is a prefix of another, so at most one
-// matches.
-__device__ __forceinline__ uint32_t exact_owner(const MatchTables& t, const uint32_t y0, const uint32_t y1) {
-    const uint64_t head = ((uint64_t)__byte_perm(y0, 0, 0x0123) << 32) | (uint64_t)__byte_perm(y1, 0, 0x0123);
+// Symbol `pos` (five bits, most significant first) of a canonical key held
+// as eight little-endian limbs, i.e. of its 32 packed bytes.
+__device__ __forceinline__ uint32_t key_symbol(const uint32_t y[8], uint32_t pos) {
+    const uint32_t bit = pos * 5, byte = bit / 8;
+    const uint32_t b0 = (y[byte / 4] >> (8 * (byte % 4))) & 0xffu;
+    const uint32_t b1 = byte + 1 < 32 ? (y[(byte + 1) / 4] >> (8 * ((byte + 1) % 4))) & 0xffu : 0u;
+    return (((b0 << 8) | b1) >> (11 - bit % 8)) & 31u;
+}
+
+// The filter a canonical key matches, or 0xffffffff: per length bucket of
+// the literal prefixes a binary search of the sorted masked heads (first 12
+// symbols at most; no kept literal is a prefix of another, so at most one
+// matches), then the patterns in order, on their key-only symbols.
+__device__ __forceinline__ uint32_t exact_owner(const MatchTables& t, const uint32_t y[8]) {
+    const uint64_t head = ((uint64_t)__byte_perm(y[0], 0, 0x0123) << 32) | (uint64_t)__byte_perm(y[1], 0, 0x0123);
     for (uint32_t b = 0; b < t.nbuckets; b++) {
         const uint64_t probe = head & (~0ULL << (64 - t.bucket_bits[b]));
         const uint64_t* k = t.keys + t.bucket_off[b];
@@ -120,6 +129,12 @@ __device__ __forceinline__ uint32_t exact_owner(const MatchTables& t, const uint
             else hi = mid;
         }
         if (lo < t.bucket_len[b] && k[lo] == probe) return t.owners[t.bucket_off[b] + lo];
+    }
+    for (uint32_t j = 0; j < t.npatterns; j++) {
+        const uint32_t* p = t.patterns + (size_t)j * PATTERN_WORDS;
+        bool ok = true;
+        for (uint32_t i = 0; i < p[1] && ok; i++) ok = (p[2 + i] >> key_symbol(y, i)) & 1u;
+        if (ok) return p[0];
     }
     return 0xffffffffu;
 }

@@ -66,10 +66,9 @@ def device_search(device, seed: bytes, prefixes, quota: int, threads: int = 0, c
             for j in idx[np.argsort(offsets[idx], kind="stable")]:
                 off, b, f = int(offsets[j]), bytes(packed[j]), int(matched[j])
                 pk, _ = key.check_hit(seed, off, b)
-                if f >= np_:
-                    if fs.match_address(pk) != f:  # a suffix: confirmed on the address
-                        continue
-                elif len(texts[f]) > 49 and not key.address(pk).startswith(texts[f]):
+                # confirmed on the full key's address: a suffix, and a prefix
+                # longer than the key-only span
+                if fs.match_address(pk) != f:
                     continue
                 found.append(Found(off, b, pk, f))
                 if len(found) == quota:

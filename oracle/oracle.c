@@ -1093,12 +1093,18 @@ double orc_chain_rate(int threads, double seconds, size_t batch, uint64_t *exami
 #define ADDRESS_LEN 56      /* src/key.rs:19 */
 
 typedef struct {
-    char canonical[ADDRESS_LEN + 1];
+    char canonical[ADDRESS_LEN * 34 + 1];
     size_t len;
     uint8_t bytes[32];
     size_t nbytes;
     uint8_t mask;
+    int pattern;           /* a prefix with `?` or `[...]`: matched by sets */
+    uint32_t sets[ADDRESS_LEN];
 } ofilter;
+
+static int parse_symbol_body(const char *s, size_t a, size_t b, uint32_t *sets, size_t *n, char *err, size_t errlen);
+static size_t render_symbol_sets(const uint32_t *sets, size_t n, char *out);
+static unsigned orc_symbol_at(const uint8_t *b, size_t len, size_t pos);
 
 struct orc_fset {
     ofilter *f;
@@ -1147,6 +1153,23 @@ static int parse_literal(const char *raw, size_t rawlen, ofilter *out, char *err
     if (n == 0) {
         snprintf(err, errlen, "the filter is empty");
         return -1;
+    }
+    out->pattern = strpbrk(body, "?[]") != NULL;
+    if (out->pattern) {
+        /* Pattern::parse with wildcards or classes (src/filter.rs:298-350,
+         * parse_symbols :495-560), anchored at the start */
+        size_t m = 0;
+        if (parse_symbol_body(body, 0, n, out->sets, &m, err, errlen) != 0) return -1;
+        int fixed = 0;
+        for (size_t i = 0; i < m; i++) fixed |= out->sets[i] != 0xffffffffu;
+        if (!fixed) {
+            snprintf(err, errlen, "nothing fixed");
+            return -1;
+        }
+        out->len = m;
+        render_symbol_sets(out->sets, m, out->canonical);
+        out->nbytes = 0;
+        return 0;
     }
     if (n > ADDRESS_LEN) {
         snprintf(err, errlen, "filter of %zu symbols is longer than an address", n);
@@ -1203,6 +1226,40 @@ static uint64_t *bitmap_build(const ofilter *f, size_t n, uint32_t bits, size_t 
     size_t nw = (size_t)(((1ULL << bits) + 63) / 64);
     uint64_t *w = calloc(nw, sizeof *w);
     for (size_t i = 0; i < n; i++) {
+        if (f[i].pattern) {
+            /* pattern_slots (src/filter.rs:2480-2530): every slot the sets
+             * allow over the window's first bits / 5 symbols and the top
+             * bits % 5 bits of the next; more than 4096 cannot be indexed */
+            uint32_t full = bits / 5, rem = bits % 5;
+            size_t nv = 1;
+            uint32_t *vals = malloc(sizeof *vals);
+            vals[0] = 0;
+            for (uint32_t k = 0; k <= full; k++) {
+                if (k == full && rem == 0) break;
+                uint32_t set = k < f[i].len ? f[i].sets[k] : 0xffffffffu;
+                uint32_t parts = 0;
+                for (unsigned v = 0; v < 32; v++)
+                    if ((set >> v) & 1) parts |= 1u << (k < full ? v : (v >> (5 - rem)));
+                size_t np = (size_t)__builtin_popcount(parts);
+                if (nv * np > 4096) {
+                    free(vals);
+                    free(w);
+                    return NULL;
+                }
+                uint32_t shift = k < full ? bits - 5 * (k + 1) : 0;
+                uint32_t *next = malloc(nv * np * sizeof *next);
+                size_t q = 0;
+                for (size_t a = 0; a < nv; a++)
+                    for (unsigned part = 0; part < 32; part++)
+                        if ((parts >> part) & 1) next[q++] = vals[a] | (part << shift);
+                free(vals);
+                vals = next;
+                nv = q;
+            }
+            for (size_t a = 0; a < nv; a++) w[vals[a] >> 6] |= 1ULL << (vals[a] & 63);
+            free(vals);
+            continue;
+        }
         size_t sym = f[i].len < KEY_ONLY_SYMBOLS ? f[i].len : KEY_ONLY_SYMBOLS;
         uint32_t pbits = (uint32_t)(sym * 5);
         uint8_t probe[32] = {0};
@@ -1243,8 +1300,20 @@ orc_fset *orc_fset_new(const char *text, uint32_t bits, char *err, size_t errlen
     /* FilterSet::new (src/filter.rs:1326-1339): sort, drop absorbed. */
     qsort(f, n, sizeof *f, cmp_canonical);
     size_t kept = 0;
+    long last_literal = -1;
     for (size_t i = 0; i < n; i++) {
-        if (kept && strncmp(f[i].canonical, f[kept - 1].canonical, f[kept - 1].len) == 0) continue;
+        if (f[i].pattern) {
+            /* patterns: exact duplicates only */
+            int dup = 0;
+            for (size_t j = 0; j < kept && !dup; j++)
+                dup = f[j].pattern && strcmp(f[j].canonical, f[i].canonical) == 0;
+            if (!dup) f[kept++] = f[i];
+            continue;
+        }
+        if (last_literal >= 0 &&
+            strncmp(f[i].canonical, f[last_literal].canonical, f[last_literal].len) == 0)
+            continue;
+        last_literal = (long)kept;
         f[kept++] = f[i];
     }
     orc_fset *s = calloc(1, sizeof *s);
@@ -1317,9 +1386,19 @@ long orc_fset_match(const orc_fset *s, const uint8_t packed[32]) {
     if (!orc_fset_may_match(s, packed)) return -1;
     for (size_t i = 0; i < s->n; i++) {
         const ofilter *f = &s->f[i];
+        if (f->pattern) continue;
         size_t last = f->nbytes - 1;
         if (memcmp(packed, f->bytes, last) == 0 && (packed[last] & f->mask) == f->bytes[last])
             return (long)i;
+    }
+    /* patterns, in order, on the key-only symbols (src/filter.rs:760-770) */
+    for (size_t i = 0; i < s->n; i++) {
+        const ofilter *f = &s->f[i];
+        if (!f->pattern) continue;
+        size_t k, m = f->len < KEY_ONLY_SYMBOLS ? f->len : KEY_ONLY_SYMBOLS;
+        for (k = 0; k < m; k++)
+            if (!((f->sets[k] >> orc_symbol_at(packed, 32, k)) & 1)) break;
+        if (k == m) return (long)i;
     }
     return -1;
 }
@@ -1390,11 +1469,10 @@ static unsigned orc_symbol_at(const uint8_t *b, size_t len, size_t pos) {
 
 /* Pattern::parse for a suffix body (src/filter.rs:298-350, parse_symbols
  * :495-560, check_reachable_tail :566-600). */
-static int parse_suffix_body(const char *s, size_t len, osuffix *out, char *err, size_t errlen) {
-    size_t a = 0, b = len;
-    while (a < b && (s[a] == ' ' || s[a] == '\t' || s[a] == '\r')) a++;
-    while (b > a && (s[b - 1] == ' ' || s[b - 1] == '\t' || s[b - 1] == '\r')) b--;
-    memset(out, 0, sizeof *out);
+/* parse_symbols (src/filter.rs:495-560): one symbol set per position,
+ * from s[a..b): a symbol, `?`, or a `[...]` class with `x-y` ranges. */
+static int parse_symbol_body(const char *s, size_t a, size_t b, uint32_t *sets, size_t *count, char *err,
+                             size_t errlen) {
     size_t n = 0;
     for (size_t i = a; i < b;) {
         uint32_t set = 0;
@@ -1428,8 +1506,37 @@ static int parse_suffix_body(const char *s, size_t len, osuffix *out, char *err,
             i++;
         }
         if (n == 56) { snprintf(err, errlen, "too long"); return -1; }
-        out->sets[n++] = set;
+        sets[n++] = set;
     }
+    *count = n;
+    return 0;
+}
+
+static size_t render_symbol_sets(const uint32_t *sets, size_t n, char *out) {
+    size_t o = 0;
+    for (size_t i = 0; i < n; i++) {
+        if (sets[i] == ORC_ALL) {
+            out[o++] = '?';
+        } else if ((sets[i] & (sets[i] - 1)) == 0) {
+            out[o++] = B32[__builtin_ctz(sets[i])];
+        } else {
+            out[o++] = '[';
+            for (int v = 0; v < 32; v++)
+                if ((sets[i] >> v) & 1) out[o++] = B32[v];
+            out[o++] = ']';
+        }
+    }
+    out[o] = 0;
+    return o;
+}
+
+static int parse_suffix_body(const char *s, size_t len, osuffix *out, char *err, size_t errlen) {
+    size_t a = 0, b = len;
+    while (a < b && (s[a] == ' ' || s[a] == '\t' || s[a] == '\r')) a++;
+    while (b > a && (s[b - 1] == ' ' || s[b - 1] == '\t' || s[b - 1] == '\r')) b--;
+    memset(out, 0, sizeof *out);
+    size_t n = 0;
+    if (parse_symbol_body(s, a, b, out->sets, &n, err, errlen) != 0) return -1;
     if (n == 0) { snprintf(err, errlen, "empty"); return -1; }
     int fixed = 0;
     for (size_t i = 0; i < n; i++) fixed |= out->sets[i] != ORC_ALL;
@@ -1442,20 +1549,7 @@ static int parse_suffix_body(const char *s, size_t len, osuffix *out, char *err,
     }
     out->len = n;
     /* a text key for sorting and de-duplication */
-    size_t o = 0;
-    for (size_t i = 0; i < n; i++) {
-        if (out->sets[i] == ORC_ALL) {
-            out->text[o++] = '?';
-        } else if ((out->sets[i] & (out->sets[i] - 1)) == 0) {
-            out->text[o++] = B32[__builtin_ctz(out->sets[i])];
-        } else {
-            out->text[o++] = '[';
-            for (int v = 0; v < 32; v++)
-                if ((out->sets[i] >> v) & 1) out->text[o++] = B32[v];
-            out->text[o++] = ']';
-        }
-    }
-    out->text[o] = 0;
+    render_symbol_sets(out->sets, n, out->text);
     return 0;
 }
 

@@ -186,3 +186,11 @@ def test_threads_argument_is_lanes(oracle, device):
     for s in survivors[:100]:
         key.check_hit(workloads.seed(0), s.offset, s.packed)
         assert fs.match_key(s.packed) is not None
+
+
+def test_paired_pattern_bitmap_survivors_equal_oracle(oracle, device):
+    """Prefixes with wildcards and classes fill the same bitmap as the
+    oracle's pattern_slots, and the same candidates survive."""
+    start, fs, got = filtered_parity(oracle, device, ["a?c", "[xyz]2", "k[a-e]?m", "q7", "mm[2-7]"], 16, 128, 2048,
+                                     8, 2)
+    assert len(got) > 100

@@ -113,3 +113,21 @@ def test_run_driver_finds_the_same_hits_with_the_device_match(device):
                                              device_match=True)
         assert len(host) == s.quota
         assert dev == host and (ex_d, adv_d) == (ex_h, adv_h)
+
+
+def test_device_match_of_patterns_equals_host_match(device):
+    """Wildcards and classes, walked on the device after the literal buckets,
+    in the same order the host's match_key walks them."""
+    start = key.start_point(workloads.seed(5))
+    fs = F.FilterSet.parse_all(["a?c", "[xyz]2", "k[a-e]?m", "q7", "mm[2-7]", "a", "[b-d]??x"])
+    words, bits = fs.index_words()
+    plain = gpu.Engine(device, start, bitmap=words, bitmap_bits=bits, config=cfg())
+    want = host_matches(plain, fs, 2)
+    plain.close()
+    matched = gpu.Engine(device, start, bitmap=words, bitmap_bits=bits, config=cfg())
+    matched.match_on_device(fs)
+    got = device_matches(matched, 2)
+    matched.close()
+    texts = fs.texts()
+    assert got == want
+    assert {texts[f] for _, _, f in got} >= {"a", "q7"} and any("?" in texts[f] or "[" in texts[f] for _, _, f in got)

@@ -106,7 +106,7 @@ def test_filter_sets_agree_with_oracle(native, oracle, filters, bits):
 def test_filter_errors(native):
     F = native.filter.FilterSet
     E = native._native.OgError
-    for bad in ["", "^", "ab0c", "a" * 57, "suffix:abd", "contains:abc", "regex:^ab", "a?c", "[ab]c"]:
+    for bad in ["", "^", "ab0c", "a" * 57, "suffix:abd", "contains:abc", "regex:^ab", "a[bc", "??"]:
         with pytest.raises(E) as e:
             F.parse_all([bad])
         assert e.value.status == "OG_E_FILTER"

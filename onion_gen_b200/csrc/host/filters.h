@@ -1,4 +1,4 @@
-// Literal address-prefix filters and the prefix bitmap the device tests.
+// Address-prefix filters and the prefix bitmap the device tests.
 //
 // Follows src/filter.rs for the prefix form: Filter::parse (bytes + mask of the
 // first min(len, 49) symbols, :649-685), FilterSet::new (sort, drop duplicates
@@ -6,8 +6,10 @@
 // packed key read big-endian, a prefix shorter than the index fills a run,
 // :2321-2604), the width choice (narrowest 16..24 at <= 1% occupancy, else the
 // widest that is <= 25% full, :2279-2295) and the exact match behind the bitmap
-// (length buckets with a binary search, :2645-2700). Wildcards, classes,
-// suffixes, substrings and regular expressions are not part of this engine.
+// (length buckets with a binary search, :2645-2700). Prefixes with `?` and
+// `[...]` classes fill the slots their symbol sets allow (pattern_slots,
+// :2480-2530) and are matched after the literals, in order. Suffixes live in
+// suffix.h; substrings and regular expressions are not part of this engine.
 #pragma once
 #include <cstddef>
 #include <cstdint>

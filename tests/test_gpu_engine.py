@@ -62,7 +62,7 @@ def test_paired_bit_exact_two_rounds(oracle, device):
     assert bad.size == 0, f"{bad.size} keys differ, first at offset {int(offs[bad[0]])}"
 
 
-@pytest.mark.parametrize("half,lanes,rounds", [(32, 256, 3), (1, 128, 2), (300, 384, 1)])
+@pytest.mark.parametrize("half,lanes,rounds", [(32, 256, 3), (1, 128, 2), (300, 384, 1), (1024, 256, 1), (2048, 128, 1)])
 def test_paired_consecutive_advances_tile_the_range(oracle, device, half, lanes, rounds):
     """Two advances continue where the first stopped: no gap, no overlap."""
     start = oracle_start(oracle, workloads.seed(7))
@@ -194,3 +194,12 @@ def test_paired_pattern_bitmap_survivors_equal_oracle(oracle, device):
     start, fs, got = filtered_parity(oracle, device, ["a?c", "[xyz]2", "k[a-e]?m", "q7", "mm[2-7]"], 16, 128, 2048,
                                      8, 2)
     assert len(got) > 100
+
+
+@pytest.mark.parametrize("bits", [8, 26])
+def test_bitmap_width_extremes(oracle, device, bits):
+    """The narrowest index the engine takes and a 64 MiB one: the same
+    survivors as the oracle's."""
+    prefixes = ["abc", "q7x"]
+    start, fs, got = filtered_parity(oracle, device, prefixes, bits, 64, 1024, 4, 4)
+    assert fs.bits == bits and len(got) > 0

@@ -326,7 +326,7 @@ void og_serve_free(og_serve* s);
  * dropped). A record's offset is 8 (w (2 half + 1) + 1 + i) with
  * w = (step / (2 half + 1)) * lanes + lane and i = step % (2 half + 1).
  *
- * Limits: lanes a multiple of 128, half <= 512, and
+ * Limits: lanes a multiple of 128, half <= 2048, and
  * lanes * (2 half + 3) * 64 + (half + 24) * 96 <= OG_NOALLOC_SCRATCH_BYTES;
  * beyond that the call fails with OG_E_CAPACITY before touching the device.
  * Work is enqueued on `stream` (a cudaStream_t; NULL for the legacy default

@@ -94,11 +94,10 @@ __global__ void __launch_bounds__(NBLOCK) noalloc_init_kernel(const NoAllocArgs 
     store_fe(a.lanes + 2 * L + lane, L, fe_mulv(Y, zi));
 }
 
-// The production paired kernel with its scratch in the file-scope array.
+// The production paired kernel with its scratch in the file-scope array; the
+// table is read through L1 as in the single engine.
 __global__ void __launch_bounds__(NBLOCK, 6) noalloc_paired_kernel(const NoAllocArgs a) {
-    extern __shared__ uint4 qtab[];
-    for (uint32_t i = threadIdx.x; i < a.half * 6; i += blockDim.x) qtab[i] = a.table[i];
-    __syncthreads();
+    const uint4* qtab = a.table;
     const uint32_t lane = blockIdx.x * blockDim.x + threadIdx.x;
     const size_t L = a.lanes_n;
     const Sink sink{a.bitmap, a.bits, a.hits, a.counter, a.cap, 0, nullptr, 0};
@@ -135,7 +134,7 @@ extern "C" int og_search_noalloc(int ordinal, const uint8_t start[128], uint32_t
     if (ordinal < 0 || ordinal >= MAX_DEVICES) return fail(err, errlen, OG_E_ARG, "device %d", ordinal);
     if (lanes == 0 || lanes % NBLOCK)
         return fail(err, errlen, OG_E_ARG, "lanes %u: a positive multiple of %u", lanes, NBLOCK);
-    if (half == 0 || half > 512) return fail(err, errlen, OG_E_ARG, "half %u outside 1..512", half);
+    if (half == 0 || half > 2048) return fail(err, errlen, OG_E_ARG, "half %u outside 1..2048", half);
     if (rounds == 0) return fail(err, errlen, OG_E_ARG, "zero rounds");
     if ((uint64_t)rounds * (2ULL * half + 1) > 0xffffffffULL) return fail(err, errlen, OG_E_ARG, "too many rounds");
     if (d_bitmap && (bits < 8 || bits > 32)) return fail(err, errlen, OG_E_ARG, "bitmap width %u outside 8..32", bits);
@@ -210,8 +209,7 @@ extern "C" int og_search_noalloc(int ordinal, const uint8_t start[128], uint32_t
     if (e != cudaSuccess) return fail(err, errlen, OG_E_DEVICE, "memset: %s", cuda_text(e).c_str());
     noalloc_table_kernel<<<(half + NBLOCK - 1) / NBLOCK, NBLOCK, 0, s>>>(a, pow8);
     noalloc_init_kernel<<<lanes / NBLOCK, NBLOCK, 0, s>>>(a);
-    const size_t smem = (size_t)half * 96;  // at most 48 KiB for half <= 512
-    noalloc_paired_kernel<<<lanes / NBLOCK, NBLOCK, smem, s>>>(a);
+    noalloc_paired_kernel<<<lanes / NBLOCK, NBLOCK, 0, s>>>(a);
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail(err, errlen, OG_E_DEVICE, "launch: %s", cuda_text(e).c_str());
     return OG_OK;

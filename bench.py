@@ -567,14 +567,20 @@ def main():
         e = gpu.Engine(dev, base, bitmap=words, bitmap_bits=bits, config=cfg)
         h2d += 128 + words.nbytes + shape.half * 96
         t_created = time.perf_counter()
-        for _ in range(e2e_steps):
-            for _ in range(advances):
-                o, k = e.advance_raw()
-                d2h += 4 + 48 * len(o)
-                matched = fs.match_many(k)
-                for j in np.nonzero(matched >= 0)[0]:
-                    key.check_hit(seed, shard.global_offset(rank, int(o[j])), bytes(k[j]))
-                    hits += 1
+        total = e2e_steps * advances
+        launched = 0
+        for i in range(total):
+            # two advances in flight: the next one runs while this one's
+            # survivors cross back and are checked
+            while launched - i < 2 and launched < total:
+                e.launch()
+                launched += 1
+            o, k = e.collect_raw()
+            d2h += 16 + 48 * len(o)
+            matched = fs.match_many(k)
+            for j in np.nonzero(matched >= 0)[0]:
+                key.check_hit(seed, shard.global_offset(rank, int(o[j])), bytes(k[j]))
+                hits += 1
         t_advanced = time.perf_counter()
         e.close()
         barrier()

@@ -109,8 +109,19 @@ void og_engine_shape(const og_engine* e, og_engine_config* cfg);
  * OG_E_OVERFLOW, never a silent truncation. */
 int og_engine_advance(og_engine* e, og_survivor* out, size_t cap, size_t* n, char* err, size_t errlen);
 
-/* Device time of the last advance's kernel, milliseconds (CUDA events on the
- * engine's stream). */
+/* The same advance in two halves, so the host can work on one advance's
+ * survivors while the next one runs: og_engine_launch enqueues an advance and
+ * returns at once; og_engine_collect waits for the oldest launched advance
+ * and returns its survivors (its records are copied on a stream of their
+ * own, beside the next advance's kernel). At most two advances are in
+ * flight (OG_E_STATE for a third launch, for a collect with none, and for
+ * og_engine_advance while launches are pending). Results come back in launch
+ * order and equal og_engine_advance's. */
+int og_engine_launch(og_engine* e, char* err, size_t errlen);
+int og_engine_collect(og_engine* e, og_survivor* out, size_t cap, size_t* n, char* err, size_t errlen);
+
+/* Device time of the last collected advance's search kernel, milliseconds
+ * (CUDA events on the engine's stream). */
 float og_engine_last_kernel_ms(const og_engine* e);
 
 /* ---- device-side exact match for the engine ------------------------------
@@ -155,6 +166,10 @@ int og_engine_new_filters(int ordinal, const uint8_t start[128], const struct og
  * first 12 on the device and confirmed on the host before they are
  * returned. */
 int og_engine_advance_matches(og_engine* e, og_match* out, size_t cap, size_t* n, char* err, size_t errlen);
+/* og_engine_advance_matches in two halves, as og_engine_launch /
+ * og_engine_collect. */
+int og_engine_launch_matches(og_engine* e, char* err, size_t errlen);
+int og_engine_collect_matches(og_engine* e, og_match* out, size_t cap, size_t* n, char* err, size_t errlen);
 
 void og_engine_free(og_engine* e);
 

@@ -139,7 +139,6 @@ uint64_t words_hash(const uint64_t* w, size_t n) {
 struct og_engine {
     int device = 0;
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     og_engine_config cfg{};
     uint32_t slots = 0;
     uint32_t bits = 0;
@@ -148,10 +147,22 @@ struct og_engine {
     float last_ms = 0;
     bool overflowed = false;
     DevBuf<uint4> lanes, scratch, table, pow2;
-    DevBuf<uint32_t> bitmap, counter;
-    DevBuf<HitRec> hits;
-    HostBuf<HitRec> h_hits;
-    HostBuf<uint32_t> h_counter;
+    DevBuf<uint32_t> bitmap;
+    // Two advances can be in flight (og_engine_launch / og_engine_collect):
+    // each has its own record buffers and counters, so the host can read one
+    // advance's results while the next one runs; the lanes and the scratch
+    // are shared, the launches being ordered on one stream.
+    struct Flight {
+        DevBuf<uint32_t> counts;  // survivors, matches, mismatched suffix keys
+        DevBuf<HitRec> hits, matches;
+        HostBuf<uint32_t> h_counts;
+        cudaEvent_t ev0 = nullptr, ev1 = nullptr, done = nullptr;
+        uint64_t launch = 0;
+        bool match = false;
+    } fl[2];
+    uint32_t head = 0, inflight = 0;
+    cudaStream_t cstream = nullptr;  // record copies, beside the next advance's kernels
+    HostBuf<HitRec> h_recs;
     PairedArgs pa{};
     ChainArgs ca{};
     uint64_t bitmap_hash = 0;  // of the bitmap the engine was created with
@@ -164,12 +175,8 @@ struct og_engine {
     uint32_t prefix_count = 0;
     og::FilterSet fs;
     DevBuf<uint64_t> mkeys;
-    DevBuf<uint32_t> mowners, mcount, mpatterns;
-    DevBuf<HitRec> matches;
-    HostBuf<HitRec> h_matches;
-    HostBuf<uint32_t> h_mcount;
-    DevBuf<uint32_t> suffixes, mismatch;
-    HostBuf<uint32_t> h_mismatch;
+    DevBuf<uint32_t> mowners, mpatterns;
+    DevBuf<uint32_t> suffixes;
     DevBuf<uint4> pow8;
     MatchArgs ma{};
 
@@ -178,8 +185,15 @@ struct og_engine {
             cudaStreamSynchronize(stream);
             cudaStreamDestroy(stream);
         }
-        if (ev0) cudaEventDestroy(ev0);
-        if (ev1) cudaEventDestroy(ev1);
+        if (cstream) {
+            cudaStreamSynchronize(cstream);
+            cudaStreamDestroy(cstream);
+        }
+        for (Flight& f : fl) {
+            if (f.ev0) cudaEventDestroy(f.ev0);
+            if (f.ev1) cudaEventDestroy(f.ev1);
+            if (f.done) cudaEventDestroy(f.done);
+        }
     }
 };
 
@@ -285,8 +299,12 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
     e->slots = slots;
     e->bits = bits;
     CU(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
-    CU(cudaEventCreate(&e->ev0));
-    CU(cudaEventCreate(&e->ev1));
+    CU(cudaStreamCreateWithFlags(&e->cstream, cudaStreamNonBlocking));
+    for (og_engine::Flight& f : e->fl) {
+        CU(cudaEventCreate(&f.ev0));
+        CU(cudaEventCreate(&f.ev1));
+        CU(cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming));
+    }
 
     const size_t L = cfg.lanes;
     const uint64_t batch = (uint64_t)L * slots * cfg.rounds;
@@ -296,10 +314,12 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
     CU(e->lanes.alloc(L * coords * 2));
     const size_t elems = cfg.scheme == OG_SCHEME_CHAIN ? cfg.half : 2 * (size_t)cfg.half + 2;
     CU(e->scratch.alloc(L * elems * 4));
-    CU(e->counter.alloc(1));
-    CU(e->hits.alloc(e->cap));
-    CU(e->h_hits.alloc(e->cap));
-    CU(e->h_counter.alloc(1));
+    for (og_engine::Flight& f : e->fl) {
+        CU(f.counts.alloc(4));
+        CU(f.hits.alloc(e->cap));
+        CU(f.h_counts.alloc(4));
+    }
+    CU(e->h_recs.alloc(e->cap));
     if (!cfg.dump && bitmap) {
         const size_t w32 = (size_t)(((1ULL << bits) + 31) / 32);
         CU(e->bitmap.alloc(std::max<size_t>(w32, 2)));
@@ -355,8 +375,8 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
         a.bits = bits;
         a.sbitmap = e->sbitmap.p;
         a.sbits = e->sbits;
-        a.hits = e->hits.p;
-        a.counter = e->counter.p;
+        a.hits = nullptr;     // set per launch to the flight's buffers
+        a.counter = nullptr;
         a.cap = (uint32_t)std::min<size_t>(e->cap, 0xffffffffu);
         a.search = 0;
         a.wx = to_words(wx);
@@ -374,8 +394,8 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
         a.bits = bits;
         a.sbitmap = e->sbitmap.p;
         a.sbits = e->sbits;
-        a.hits = e->hits.p;
-        a.counter = e->counter.p;
+        a.hits = nullptr;     // set per launch to the flight's buffers
+        a.counter = nullptr;
         a.cap = (uint32_t)std::min<size_t>(e->cap, 0xffffffffu);
         a.search = 0;
         a.step_ypx = to_words(step.ypx);
@@ -450,12 +470,7 @@ int enable_matching(og_engine* e, const og_filters* f, char* err, size_t errlen)
         CU(e->pow8.alloc(pw.size()));
         CU(cudaMemcpyAsync(e->pow8.p, pw.data(), pw.size() * sizeof(uint4), cudaMemcpyHostToDevice, e->stream));
     }
-    CU(e->mcount.alloc(1));
-    CU(e->h_mcount.alloc(1));
-    CU(e->mismatch.alloc(1));
-    CU(e->h_mismatch.alloc(1));
-    CU(e->matches.alloc(e->cap));
-    CU(e->h_matches.alloc(e->cap));
+    for (og_engine::Flight& fl : e->fl) CU(fl.matches.alloc(e->cap));
     CU(cudaStreamSynchronize(e->stream));
     e->fs = f->set;
     e->long_filters = false;
@@ -466,8 +481,8 @@ int enable_matching(og_engine* e, const og_filters* f, char* err, size_t errlen)
     e->prefix_count = f->has_prefixes ? (uint32_t)f->set.size() : 0;
     MatchArgs& m = e->ma;
     m = MatchArgs{};
-    m.surv = e->hits.p;
-    m.surv_count = e->counter.p;
+    m.surv = nullptr;  // the flight's buffers, set per launch
+    m.surv_count = nullptr;
     m.surv_cap = (uint32_t)std::min<size_t>(e->cap, 0xffffffffu);
     m.t = match_tables(buckets, e->mkeys.p, e->mowners.p, e->mpatterns.p,
                        (uint32_t)(pats.size() / FilterSet::PATTERN_ROW));
@@ -484,14 +499,91 @@ int enable_matching(og_engine* e, const og_filters* f, char* err, size_t errlen)
     m.lanes = e->cfg.lanes;
     m.slots = e->slots;
     m.paired = e->cfg.scheme == OG_SCHEME_PAIRED ? 1u : 0u;
-    m.out = e->matches.p;
-    m.out_count = e->mcount.p;
+    m.out = nullptr;
+    m.out_count = nullptr;
     m.out_cap = m.surv_cap;
-    m.mismatch = e->mismatch.p;
+    m.mismatch = nullptr;
     e->matching = true;
     return OG_OK;
 }
 
+
+// One advance onto the engine's stream, into the next free flight: the
+// search kernel, optionally the device match, and the copy of the counters.
+int enqueue_advance(og_engine* e, bool match, char* err, size_t errlen) {
+    if (!e) return fail(err, errlen, OG_E_ARG, "null argument");
+    if (e->overflowed) return fail(err, errlen, OG_E_STATE, "an earlier advance overflowed; the engine is closed");
+    if (e->inflight == 2) return fail(err, errlen, OG_E_STATE, "two advances are in flight: collect one first");
+    og_engine::Flight& f = e->fl[(e->head + e->inflight) & 1];
+    CU(cudaSetDevice(e->device));
+    CU(cudaMemsetAsync(f.counts.p, 0, 4 * sizeof(uint32_t), e->stream));
+    CU(cudaEventRecord(f.ev0, e->stream));
+    if (e->cfg.scheme == OG_SCHEME_PAIRED) {
+        e->pa.hits = f.hits.p;
+        e->pa.counter = f.counts.p;
+        CU(launch_paired(e->pa, (int)e->cfg.block, e->stream));
+    } else {
+        e->ca.hits = f.hits.p;
+        e->ca.counter = f.counts.p;
+        CU(launch_chain(e->ca, (int)e->cfg.block, e->stream));
+    }
+    CU(cudaEventRecord(f.ev1, e->stream));
+    if (match) {
+        MatchArgs& m = e->ma;
+        m.surv = f.hits.p;
+        m.surv_count = f.counts.p;
+        m.out = f.matches.p;
+        m.out_count = f.counts.p + 1;
+        m.mismatch = f.counts.p + 2;
+        m.window0 = e->launches * (uint64_t)e->cfg.rounds * e->cfg.lanes;
+        int sms = 0;
+        CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device));
+        CU(launch_match(m, std::max(sms, 1) * 4, e->stream));
+    }
+    CU(cudaMemcpyAsync(f.h_counts.p, f.counts.p, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream));
+    CU(cudaEventRecord(f.done, e->stream));
+    f.launch = e->launches++;
+    f.match = match;
+    e->inflight++;
+    return OG_OK;
+}
+
+// Waits for the oldest flight and copies its records (survivors, or matches
+// for a matching flight) into h_recs on the copy stream, beside whatever
+// advance runs next. The flight is released whatever happens.
+int collect_flight(og_engine* e, bool match, uint32_t* count, uint64_t* launch, char* err, size_t errlen) {
+    if (e->inflight == 0) return fail(err, errlen, OG_E_STATE, "no advance in flight");
+    og_engine::Flight& f = e->fl[e->head];
+    if (f.match != match)
+        return fail(err, errlen, OG_E_STATE, "the oldest advance in flight was launched %s the device match",
+                    f.match ? "with" : "without");
+    e->head ^= 1;
+    e->inflight--;
+    CU(cudaSetDevice(e->device));
+    CU(cudaEventSynchronize(f.done));
+    cudaEventElapsedTime(&e->last_ms, f.ev0, f.ev1);
+    *launch = f.launch;
+    const uint32_t found = f.h_counts.p[0];
+    if (found > e->cap) {
+        e->overflowed = true;
+        return fail(err, errlen, OG_E_OVERFLOW,
+                    "one advance produced %u survivors and only %zu fit; the index is too narrow for what it "
+                    "is filtering: a wider index is the answer",
+                    found, e->cap);
+    }
+    if (match && f.h_counts.p[2])
+        return fail(err, errlen, OG_E_VERIFY,
+                    "%u survivors' keys recomputed from their offsets differ from the search kernel's",
+                    f.h_counts.p[2]);
+    const uint32_t n = match ? f.h_counts.p[1] : found;  // matches are at most the survivors
+    if (n) {
+        CU(cudaMemcpyAsync(e->h_recs.p, match ? f.matches.p : f.hits.p, (size_t)n * sizeof(HitRec),
+                           cudaMemcpyDeviceToHost, e->cstream));
+        CU(cudaStreamSynchronize(e->cstream));
+    }
+    *count = n;
+    return OG_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -620,41 +712,20 @@ void og_engine_shape(const og_engine* e, og_engine_config* cfg) {
 
 float og_engine_last_kernel_ms(const og_engine* e) { return e ? e->last_ms : 0.f; }
 
-int og_engine_advance(og_engine* e, og_survivor* out, size_t cap, size_t* n, char* err, size_t errlen) {
+int og_engine_launch(og_engine* e, char* err, size_t errlen) { return enqueue_advance(e, false, err, errlen); }
+
+int og_engine_collect(og_engine* e, og_survivor* out, size_t cap, size_t* n, char* err, size_t errlen) {
     if (!e || !n) return fail(err, errlen, OG_E_ARG, "null argument");
     *n = 0;
-    if (e->overflowed) return fail(err, errlen, OG_E_STATE, "an earlier advance overflowed; the engine is closed");
-    CU(cudaSetDevice(e->device));
-    CU(cudaMemsetAsync(e->counter.p, 0, sizeof(uint32_t), e->stream));
-    CU(cudaEventRecord(e->ev0, e->stream));
-    if (e->cfg.scheme == OG_SCHEME_PAIRED) {
-        CU(launch_paired(e->pa, (int)e->cfg.block, e->stream));
-    } else {
-        CU(launch_chain(e->ca, (int)e->cfg.block, e->stream));
-    }
-    CU(cudaEventRecord(e->ev1, e->stream));
-    CU(cudaMemcpyAsync(e->h_counter.p, e->counter.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream));
-    CU(cudaStreamSynchronize(e->stream));
-    cudaEventElapsedTime(&e->last_ms, e->ev0, e->ev1);
-    const uint64_t launch = e->launches++;
-    const uint32_t found = *e->h_counter.p;
-    if (found > e->cap) {
-        e->overflowed = true;
-        return fail(err, errlen, OG_E_OVERFLOW,
-                    "one advance produced %u survivors and only %zu fit; the index is too narrow for what it "
-                    "is filtering: a wider index is the answer",
-                    found, e->cap);
-    }
-    if (found > cap)
-        return fail(err, errlen, OG_E_CAPACITY, "%u survivors and room for %zu in the caller's buffer", found, cap);
-    if (found) {
-        CU(cudaMemcpyAsync(e->h_hits.p, e->hits.p, (size_t)found * sizeof(HitRec), cudaMemcpyDeviceToHost, e->stream));
-        CU(cudaStreamSynchronize(e->stream));
-    }
+    uint32_t found = 0;
+    uint64_t launch = 0;
+    int rc = collect_flight(e, false, &found, &launch, err, errlen);
+    if (rc != OG_OK) return rc;
+    if (found > cap) return fail(err, errlen, OG_E_CAPACITY, "%u survivors and room for %zu in the caller's buffer", found, cap);
     const uint64_t L = e->cfg.lanes, slots = e->slots, R = e->cfg.rounds;
     const bool paired = e->cfg.scheme == OG_SCHEME_PAIRED;
     for (uint32_t k = 0; k < found; k++) {
-        const HitRec& h = e->h_hits.p[k];
+        const HitRec& h = e->h_recs.p[k];
         const uint64_t r = h.step / slots, i = h.step % slots;
         const uint64_t w = (launch * R + r) * L + h.lane;
         out[k].offset = paired ? 8 * (w * slots + 1 + i) : 8 * (w * slots + i);
@@ -667,6 +738,15 @@ int og_engine_advance(og_engine* e, og_survivor* out, size_t cap, size_t* n, cha
     }
     *n = found;
     return OG_OK;
+}
+
+int og_engine_advance(og_engine* e, og_survivor* out, size_t cap, size_t* n, char* err, size_t errlen) {
+    if (!e || !n) return fail(err, errlen, OG_E_ARG, "null argument");
+    *n = 0;
+    if (e->inflight) return fail(err, errlen, OG_E_STATE, "launched advances are not collected yet");
+    const int rc = og_engine_launch(e, err, errlen);
+    if (rc != OG_OK) return rc;
+    return og_engine_collect(e, out, cap, n, err, errlen);
 }
 
 int og_engine_match_on_device(og_engine* e, const og_filters* f, char* err, size_t errlen) {
@@ -684,55 +764,23 @@ int og_engine_match_on_device(og_engine* e, const og_filters* f, char* err, size
     return enable_matching(e, f, err, errlen);
 }
 
-int og_engine_advance_matches(og_engine* e, og_match* out, size_t cap, size_t* n, char* err, size_t errlen) {
+int og_engine_launch_matches(og_engine* e, char* err, size_t errlen) {
+    if (e && !e->matching) return fail(err, errlen, OG_E_STATE, "og_engine_match_on_device has not been called");
+    return enqueue_advance(e, true, err, errlen);
+}
+
+int og_engine_collect_matches(og_engine* e, og_match* out, size_t cap, size_t* n, char* err, size_t errlen) {
     if (!e || !n) return fail(err, errlen, OG_E_ARG, "null argument");
     *n = 0;
-    if (!e->matching) return fail(err, errlen, OG_E_STATE, "og_engine_match_on_device has not been called");
-    if (e->overflowed) return fail(err, errlen, OG_E_STATE, "an earlier advance overflowed; the engine is closed");
-    CU(cudaSetDevice(e->device));
-    CU(cudaMemsetAsync(e->counter.p, 0, sizeof(uint32_t), e->stream));
-    CU(cudaMemsetAsync(e->mcount.p, 0, sizeof(uint32_t), e->stream));
-    CU(cudaMemsetAsync(e->mismatch.p, 0, sizeof(uint32_t), e->stream));
-    e->ma.window0 = e->launches * (uint64_t)e->cfg.rounds * e->cfg.lanes;
-    CU(cudaEventRecord(e->ev0, e->stream));
-    if (e->cfg.scheme == OG_SCHEME_PAIRED) {
-        CU(launch_paired(e->pa, (int)e->cfg.block, e->stream));
-    } else {
-        CU(launch_chain(e->ca, (int)e->cfg.block, e->stream));
-    }
-    CU(cudaEventRecord(e->ev1, e->stream));
-    int sms = 0;
-    CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device));
-    CU(launch_match(e->ma, std::max(sms, 1) * 4, e->stream));
-    CU(cudaMemcpyAsync(e->h_counter.p, e->counter.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream));
-    CU(cudaMemcpyAsync(e->h_mcount.p, e->mcount.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream));
-    CU(cudaMemcpyAsync(e->h_mismatch.p, e->mismatch.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream));
-    CU(cudaStreamSynchronize(e->stream));
-    cudaEventElapsedTime(&e->last_ms, e->ev0, e->ev1);
-    const uint64_t launch = e->launches++;
-    const uint32_t found = *e->h_counter.p;
-    if (found > e->cap) {
-        e->overflowed = true;
-        return fail(err, errlen, OG_E_OVERFLOW,
-                    "one advance produced %u survivors and only %zu fit; the index is too narrow for what it "
-                    "is filtering: a wider index is the answer",
-                    found, e->cap);
-    }
-    if (*e->h_mismatch.p)
-        return fail(err, errlen, OG_E_VERIFY,
-                    "%u survivors' keys recomputed from their offsets differ from the search kernel's",
-                    *e->h_mismatch.p);
-    const uint32_t matched = *e->h_mcount.p;  // at most `found`, so within the buffer
-    if (matched) {
-        CU(cudaMemcpyAsync(e->h_matches.p, e->matches.p, (size_t)matched * sizeof(HitRec), cudaMemcpyDeviceToHost,
-                           e->stream));
-        CU(cudaStreamSynchronize(e->stream));
-    }
+    uint32_t matched = 0;
+    uint64_t launch = 0;
+    int rc = collect_flight(e, true, &matched, &launch, err, errlen);
+    if (rc != OG_OK) return rc;
     const uint64_t L = e->cfg.lanes, slots = e->slots, R = e->cfg.rounds;
     const bool paired = e->cfg.scheme == OG_SCHEME_PAIRED;
     size_t k = 0;
     for (uint32_t j = 0; j < matched; j++) {
-        const HitRec& h = e->h_matches.p[j];
+        const HitRec& h = e->h_recs.p[j];
         og_match m;
         std::memset(&m, 0, sizeof m);
         for (int q = 0; q < 8; q++)
@@ -756,6 +804,15 @@ int og_engine_advance_matches(og_engine* e, og_match* out, size_t cap, size_t* n
     }
     *n = k;
     return OG_OK;
+}
+
+int og_engine_advance_matches(og_engine* e, og_match* out, size_t cap, size_t* n, char* err, size_t errlen) {
+    if (!e || !n) return fail(err, errlen, OG_E_ARG, "null argument");
+    *n = 0;
+    if (e->inflight) return fail(err, errlen, OG_E_STATE, "launched advances are not collected yet");
+    const int rc = og_engine_launch_matches(e, err, errlen);
+    if (rc != OG_OK) return rc;
+    return og_engine_collect_matches(e, out, cap, n, err, errlen);
 }
 
 void og_engine_free(og_engine* e) { delete e; }

@@ -145,6 +145,25 @@ class Engine:
         offsets, packed = self.advance_raw()
         return [Survivor(int(o), bytes(p)) for o, p in zip(offsets, packed)]
 
+    def launch(self):
+        """og_engine_launch: enqueue one advance and return at once (at most
+        two in flight)."""
+        err = N.errbuf()
+        N.check(N.lib.og_engine_launch(self._h, err, 512), err)
+
+    def collect_raw(self):
+        """og_engine_collect: the oldest launched advance's survivors, as
+        advance_raw returns them."""
+        n = C.c_size_t()
+        err = N.errbuf()
+        N.check(N.lib.og_engine_collect(self._h, self._buf, self._room, C.byref(n), err, 512), err)
+        return self._survivors(n.value)
+
+    def _survivors(self, k):
+        raw = np.frombuffer(self._buf, dtype=np.uint8, count=k * 40).reshape(k, 40)
+        offsets = raw[:, :8].copy().view(np.uint64).reshape(k)
+        return offsets, raw[:, 8:40].copy()
+
     def match_on_device(self, filters):
         """Exact match on the device from now on (og_engine_match_on_device):
         ``filters`` is the ``filter.FilterSet`` whose index_words this engine
@@ -161,7 +180,21 @@ class Engine:
         n = C.c_size_t()
         err = N.errbuf()
         N.check(N.lib.og_engine_advance_matches(self._h, self._mbuf, self._room, C.byref(n), err, 512), err)
-        k = n.value
+        return self._matches(n.value)
+
+    def launch_matches(self):
+        """og_engine_launch_matches: enqueue one advance with the device match."""
+        err = N.errbuf()
+        N.check(N.lib.og_engine_launch_matches(self._h, err, 512), err)
+
+    def collect_matches_raw(self):
+        """og_engine_collect_matches: the oldest launched advance's matches."""
+        n = C.c_size_t()
+        err = N.errbuf()
+        N.check(N.lib.og_engine_collect_matches(self._h, self._mbuf, self._room, C.byref(n), err, 512), err)
+        return self._matches(n.value)
+
+    def _matches(self, k):
         raw = np.frombuffer(self._mbuf, dtype=np.uint8, count=k * 48).reshape(k, 48)
         offsets = raw[:, :8].copy().view(np.uint64).reshape(k)
         filters = raw[:, 40:44].copy().view(np.uint32).reshape(k)

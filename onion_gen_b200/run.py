@@ -48,15 +48,21 @@ def device_search(device, seed: bytes, prefixes, quota: int, threads: int = 0, c
     found = []
     advances = 0
     examined = 0
+    launch = eng.launch_matches if device_match else eng.launch
+    launched = 0
     try:
         while len(found) < quota:
             if max_advances is not None and advances >= max_advances:
                 break
+            # keep the next advance running while this one is checked
+            while launched - advances < 2 and (max_advances is None or launched < max_advances):
+                launch()
+                launched += 1
             if device_match:
-                offsets, packed, matched = eng.advance_matches_raw()
+                offsets, packed, matched = eng.collect_matches_raw()
                 idx = np.arange(len(offsets))
             else:
-                offsets, packed = eng.advance_raw()
+                offsets, packed = eng.collect_raw()
                 matched = fs.match_many(packed)  # the bitmap says maybe, the exact check decides
                 idx = np.nonzero(matched >= 0)[0]
             advances += 1

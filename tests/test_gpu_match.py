@@ -131,3 +131,50 @@ def test_device_match_of_patterns_equals_host_match(device):
     texts = fs.texts()
     assert got == want
     assert {texts[f] for _, _, f in got} >= {"a", "q7"} and any("?" in texts[f] or "[" in texts[f] for _, _, f in got)
+
+
+def test_launch_and_collect_pipeline_equals_advance(device):
+    """Two advances in flight (og_engine_launch / og_engine_collect) give the
+    same survivors, in launch order, as advance after advance; so do the
+    matching halves; misuse is an error, not a hang."""
+    start = key.start_point(workloads.seed(6))
+    fs = F.FilterSet.parse_all(["ab", "x7", "suffix:" + "b" * 7 + "qd"])
+    a = gpu.Engine(device, start, filters=fs, config=cfg())
+    want = [a.advance_raw() for _ in range(4)]
+    a.close()
+    b = gpu.Engine(device, start, filters=fs, config=cfg())
+    with pytest.raises(N.OgError) as e:
+        b.collect_raw()
+    assert e.value.status == "OG_E_STATE"
+    got = []
+    b.launch()
+    b.launch()
+    with pytest.raises(N.OgError) as e:
+        b.launch()
+    assert e.value.status == "OG_E_STATE"
+    with pytest.raises(N.OgError) as e:
+        b.advance_raw()
+    assert e.value.status == "OG_E_STATE"
+    got.append(b.collect_raw())
+    b.launch()
+    got.append(b.collect_raw())
+    got.append(b.collect_raw())
+    b.launch()
+    got.append(b.collect_raw())
+    for (wo, wk), (go, gk) in zip(want, got):
+        assert np.array_equal(wo, go) and np.array_equal(wk, gk)
+    b.close()
+    # the matching halves
+    c = gpu.Engine(device, start, filters=fs, config=cfg())
+    want = [c.advance_matches_raw() for _ in range(3)]
+    c.close()
+    d = gpu.Engine(device, start, filters=fs, config=cfg())
+    d.launch_matches()
+    d.launch_matches()
+    got = [d.collect_matches_raw()]
+    d.launch_matches()
+    got += [d.collect_matches_raw(), d.collect_matches_raw()]
+    for w, g in zip(want, got):
+        assert all(np.array_equal(x, y) for x, y in zip(w, g))
+    assert sum(len(w[0]) for w in want) > 0
+    d.close()

@@ -414,8 +414,13 @@ def suffix_leg(dev, steps, advances):
     matches = verified = 0
     kernel_ms = 0.0
     t0 = time.perf_counter()
-    for _ in range(steps * advances):
-        o, k, f = eng.advance_matches_raw()
+    total = steps * advances
+    launched = 0
+    for i in range(total):
+        while launched - i < 2 and launched < total:
+            eng.launch_matches()
+            launched += 1
+        o, k, f = eng.collect_matches_raw()
         kernel_ms += eng.last_kernel_ms()
         for off, packed, fi in zip(o, k, f):
             pk, _ = key.check_hit(seed, int(off), bytes(packed))

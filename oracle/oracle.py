@@ -314,9 +314,9 @@ class FilterSet:
 
     def canonical(self):
         out = []
-        b = _buf(64)
+        b = _buf(4096)
         for i in range(len(self)):
-            lib().orc_fset_canonical(self._h, i, b, 64)
+            lib().orc_fset_canonical(self._h, i, b, 4096)
             out.append(b.value.decode())
         return out
 

@@ -76,3 +76,37 @@ def test_pattern_full_address_check():
     assert fs.match_address(pk) == 0
     wrong = addr[:10] + "?" + addr[11:50] + ("b" if addr[50] != "b" else "c")
     assert F.FilterSet.parse_all([wrong]).match_address(pk) is None
+
+
+def test_random_pattern_sets_against_the_oracle(oracle):
+    """Seeded random mixes of literals, wildcards and classes: accepted or
+    refused alike, the same kept set and bitmap, the same matches."""
+    import random
+
+    rng = random.Random(1)
+
+    def sym():
+        r = rng.random()
+        if r < 0.7:
+            return rng.choice(ALPHABET)
+        if r < 0.85:
+            return "?"
+        a, b = sorted(rng.sample(range(32), 2))
+        return "[" + (ALPHABET[a] + "-" + ALPHABET[b] if rng.random() < 0.5 else "".join(rng.sample(ALPHABET, 3))) + "]"
+
+    for trial in range(60):
+        filters = ["".join(sym() for _ in range(rng.randint(2, 9))) for _ in range(rng.randint(1, 6))]
+        bits = rng.choice([0, 16, 20])
+        try:
+            fs = F.FilterSet.parse_all(filters, bits=bits)
+        except N.OgError:
+            with pytest.raises(ValueError):
+                oracle.FilterSet(filters, bits=bits)
+            continue
+        o = oracle.FilterSet(filters, bits=bits)
+        assert fs.texts() == o.canonical() and fs.bits == o.bits
+        assert np.array_equal(fs.index_words()[0], o.words())
+        keys = np.random.default_rng(trial).integers(0, 256, (2000, 32), dtype=np.uint8)
+        keys[:, 31] &= 0x7F
+        want = np.array([o.match(bytes(k)) for k in keys], dtype=np.int32)
+        assert np.array_equal(fs.match_many(keys), want)

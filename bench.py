@@ -56,7 +56,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 CANDIDATES_PER_STEP = 1 << 32
-HALF = 1024
+HALF = 2048
 # the plain engine of the batched leg (one search at a time) and the batch's
 # profiling case: a short round, so that small searches do not overshoot
 SHORT_HALF = 256

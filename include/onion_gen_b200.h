@@ -80,8 +80,12 @@ enum og_scheme {
 /* Launch shape of an engine. Zero fields take defaults. */
 typedef struct og_engine_config {
     uint32_t scheme;   /* og_scheme */
-    uint32_t half;     /* paired: table size; a round is 2*half+1 candidates. chain: n steps */
-    uint32_t lanes;    /* lanes (independent chains), a multiple of `block` */
+    uint32_t half;     /* paired: table size, a round is 2*half+1 candidates (0: 2048).
+                          chain: n steps (0: 1024) */
+    uint32_t lanes;    /* lanes (independent chains), a multiple of `block`. The paired
+                          kernel runs as many CTAs as are resident and they take the lanes
+                          a block at a time, so its scratch is that of the resident CTAs
+                          whatever the lanes (0: eight blocks per resident CTA) */
     uint32_t rounds;   /* rounds per advance */
     uint32_t block;    /* threads per CUDA block, a multiple of 32 */
     uint32_t dump;     /* 1: ignore the bitmap, every candidate survives (parity runs) */

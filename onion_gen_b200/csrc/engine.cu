@@ -142,6 +142,7 @@ struct og_engine {
     og_engine_config cfg{};
     uint32_t slots = 0;
     uint32_t bits = 0;
+    uint32_t grid = 0;  // persistent CTAs of the paired kernel
     size_t cap = 0;
     uint64_t launches = 0;
     float last_ms = 0;
@@ -258,35 +259,47 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
     if (cfg.block == 0) cfg.block = 128;
     if (cfg.block % 32 || cfg.block > OG_LB_THREADS)
         return fail(err, errlen, OG_E_ARG, "block %u (a multiple of 32, at most %d)", cfg.block, OG_LB_THREADS);
-    if (cfg.half == 0) cfg.half = 1024;
+    if (cfg.half == 0) cfg.half = cfg.scheme == OG_SCHEME_CHAIN ? 1024 : 2048;
     if (cfg.scheme == OG_SCHEME_PAIRED && cfg.half > 2048) return fail(err, errlen, OG_E_ARG, "half %u > 2048", cfg.half);
     if (cfg.scheme == OG_SCHEME_CHAIN && cfg.half > 65536) return fail(err, errlen, OG_E_ARG, "n %u > 65536", cfg.half);
+    const uint32_t slots = cfg.scheme == OG_SCHEME_CHAIN ? cfg.half : 2 * cfg.half + 1;
+    double occ = 1.0;  // the share of candidates the bitmaps let through
+    if (!cfg.dump) {
+        occ = 0.0;
+        if (bitmap) {
+            std::vector<uint64_t> w(bitmap, bitmap + (size_t)(((1ULL << bits) + 63) / 64));
+            occ = bitmap_occupancy(w, bits);
+        }
+        if (suffixed) occ += f->suffixes.occupancy();
+    }
     if (cfg.lanes == 0) {
-        // two waves of resident blocks: measured 5% ahead of one, as the
-        // second wave overlaps the first's tail
-        int rc = resident_lanes(ordinal, cfg.scheme, cfg.half, cfg.block, &cfg.lanes, err, errlen);
+        uint32_t resident = 0;
+        int rc = resident_lanes(ordinal, cfg.scheme, cfg.half, cfg.block, &resident, err, errlen);
         if (rc) return rc;
-        cfg.lanes *= 2;
+        if (cfg.scheme == OG_SCHEME_PAIRED) {
+            // the persistent kernel takes lanes a block at a time: eight
+            // blocks per resident CTA leave the last ones little tail
+            // (measured +3.5% over two), while the scratch stays that of the
+            // resident CTAs; fewer when the survivor buffer of one advance
+            // would pass 2^24 records
+            uint32_t waves = 8;
+            while (waves > 1 && 4.0 * (double)resident * waves * slots * occ > (double)(1u << 24)) waves /= 2;
+            cfg.lanes = resident * waves;
+        } else {
+            // two waves of resident blocks: the second overlaps the first's tail
+            cfg.lanes = resident * 2;
+        }
     }
     cfg.lanes = (cfg.lanes + cfg.block - 1) / cfg.block * cfg.block;
     if (cfg.lanes > (1u << 24)) return fail(err, errlen, OG_E_ARG, "%u lanes (at most 2^24)", cfg.lanes);
-    const uint32_t slots = cfg.scheme == OG_SCHEME_CHAIN ? cfg.half : 2 * cfg.half + 1;
     if (cfg.rounds == 0) {
         const uint64_t per_round = (uint64_t)cfg.lanes * slots;
         cfg.rounds = (uint32_t)std::max<uint64_t>(1, (1ULL << 27) / per_round);
     }
-    double occupancy = 1.0;
-    if (!cfg.dump) {
-        occupancy = 0.0;
-        if (bitmap) {
-            std::vector<uint64_t> w(bitmap, bitmap + (size_t)(((1ULL << bits) + 63) / 64));
-            occupancy = bitmap_occupancy(w, bits);
-        }
-        if (suffixed) occupancy += f->suffixes.occupancy();
-        // keep the survivor buffer of one advance within 2^24 records
-        while (cfg.rounds > 1 && 4.0 * (double)cfg.lanes * slots * cfg.rounds * occupancy > (double)(1u << 24))
-            cfg.rounds /= 2;
-    }
+    const double occupancy = occ;
+    // keep the survivor buffer of one advance within 2^24 records
+    while (!cfg.dump && cfg.rounds > 1 && 4.0 * (double)cfg.lanes * slots * cfg.rounds * occupancy > (double)(1u << 24))
+        cfg.rounds /= 2;
     if ((uint64_t)cfg.rounds * slots > 0xffffffffULL) return fail(err, errlen, OG_E_ARG, "too many rounds per advance");
 
     Pt start_pt = point_from_bytes(start);
@@ -313,7 +326,16 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
     const uint32_t coords = cfg.scheme == OG_SCHEME_CHAIN ? 4 : 2;
     CU(e->lanes.alloc(L * coords * 2));
     const size_t elems = cfg.scheme == OG_SCHEME_CHAIN ? cfg.half : 2 * (size_t)cfg.half + 2;
-    CU(e->scratch.alloc(L * elems * 4));
+    if (cfg.scheme == OG_SCHEME_PAIRED) {
+        // the paired kernel is persistent: scratch for the resident CTAs only
+        uint32_t resident = 0;
+        int rc = resident_lanes(ordinal, cfg.scheme, cfg.half, cfg.block, &resident, err, errlen);
+        if (rc) return rc;
+        e->grid = std::max<uint32_t>(1, resident / cfg.block);
+        CU(e->scratch.alloc((size_t)e->grid * cfg.block * elems * 4));
+    } else {
+        CU(e->scratch.alloc(L * elems * 4));
+    }
     for (og_engine::Flight& f : e->fl) {
         CU(f.counts.alloc(4));
         CU(f.hits.alloc(e->cap));
@@ -371,6 +393,8 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
         a.table = e->table.p;
         a.lanes = e->lanes.p;
         a.scratch = e->scratch.p;
+        a.work = nullptr;  // the flight's counter, set per launch
+        a.slots_n = e->grid * cfg.block;
         a.bitmap = cfg.dump ? nullptr : e->bitmap.p;
         a.bits = bits;
         a.sbitmap = e->sbitmap.p;
@@ -521,7 +545,8 @@ int enqueue_advance(og_engine* e, bool match, char* err, size_t errlen) {
     if (e->cfg.scheme == OG_SCHEME_PAIRED) {
         e->pa.hits = f.hits.p;
         e->pa.counter = f.counts.p;
-        CU(launch_paired(e->pa, (int)e->cfg.block, e->stream));
+        e->pa.work = f.counts.p + 3;
+        CU(launch_paired(e->pa, (int)e->cfg.block, (int)e->grid, e->stream));
     } else {
         e->ca.hits = f.hits.p;
         e->ca.counter = f.counts.p;
@@ -660,10 +685,10 @@ int og_engine_new(int ordinal, const uint8_t start[128], uint32_t threads, const
     og_engine* best = nullptr;
     double best_rate = -1;
     int last = OG_E_DEVICE;
-    for (uint32_t half : {256u, 512u, 1024u}) {
+    for (uint32_t half : {512u, 1024u, 2048u}) {
         uint32_t resident = 0;
         if (resident_lanes(ordinal, OG_SCHEME_PAIRED, half, 128, &resident, err, errlen) != OG_OK) continue;
-        for (uint32_t mult : {1u, 2u, 3u}) {
+        for (uint32_t mult : {2u, 4u, 8u}) {
             og_engine_config c{};
             c.scheme = OG_SCHEME_PAIRED;
             c.half = half;

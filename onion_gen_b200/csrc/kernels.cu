@@ -50,16 +50,27 @@ __global__ void __launch_bounds__(OG_LB_THREADS, OG_LB_MIN_BLOCKS) paired_kernel
     // large tables from capping occupancy (measured 17.97 vs 13.3 G keys/s
     // at half 1024, and the same speed at half 256).
     const uint4* qtab = a.table;
-
-    const uint32_t lane = blockIdx.x * blockDim.x + threadIdx.x;
-    const size_t L = a.lanes_n;
+    // Persistent: each CTA takes the next block of lanes until none is left.
+    // The scratch is indexed by the CTA's slot, not the lane.
+    __shared__ uint32_t item_s;
+    const size_t L = a.lanes_n, S = a.slots_n;
+    const uint32_t nblocks = a.lanes_n / blockDim.x;
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     const Sink sink{a.bitmap, a.bits, a.hits, a.counter, a.cap, a.search, a.sbitmap, a.sbits};
-    fe x = load_fe(a.lanes + 0 * L + lane, L);
-    fe y = load_fe(a.lanes + 2 * L + lane, L);
-    paired_rounds(x, y, words_fe(a.wx), words_fe(a.wy), words_fe(a.wt), qtab, a.half, a.rounds, a.scratch + lane, L,
-                  [&](const fe& v, uint32_t step) { test_emit(sink, v, lane, step); });
-    store_fe(a.lanes + 0 * L + lane, L, x);
-    store_fe(a.lanes + 2 * L + lane, L, y);
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) item_s = atomicAdd(a.work, 1u);
+        __syncthreads();
+        const uint32_t item = item_s;
+        if (item >= nblocks) break;
+        const uint32_t lane = item * blockDim.x + threadIdx.x;
+        fe x = load_fe(a.lanes + 0 * L + lane, L);
+        fe y = load_fe(a.lanes + 2 * L + lane, L);
+        paired_rounds(x, y, words_fe(a.wx), words_fe(a.wy), words_fe(a.wt), qtab, a.half, a.rounds, a.scratch + slot, S,
+                      [&](const fe& v, uint32_t step) { test_emit(sink, v, lane, step); });
+        store_fe(a.lanes + 0 * L + lane, L, x);
+        store_fe(a.lanes + 2 * L + lane, L, y);
+    }
 }
 
 // the chain kernel (parity contract, not the production path) keeps 96 registers: at 80 it spills
@@ -148,9 +159,10 @@ cudaError_t launch_init(const InitArgs& a, int block, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_paired(const PairedArgs& a, int block, cudaStream_t s) {
-    if (a.lanes_n % block != 0 || block % 32 != 0) return cudaErrorInvalidValue;
-    paired_kernel<<<a.lanes_n / block, block, 0, s>>>(a);
+cudaError_t launch_paired(const PairedArgs& a, int block, int grid, cudaStream_t s) {
+    if (a.lanes_n % block != 0 || block % 32 != 0 || grid <= 0 || a.slots_n != (uint32_t)grid * (uint32_t)block)
+        return cudaErrorInvalidValue;
+    paired_kernel<<<grid, block, 0, s>>>(a);
     return cudaGetLastError();
 }
 

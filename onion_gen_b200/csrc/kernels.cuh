@@ -47,7 +47,9 @@ struct FeWords {
 struct PairedArgs {
     const uint4* table;      // Q_m, m = 1..half: ((m-1)*3 + {x,y,t}) * 2 + q
     uint4* lanes;            // affine centres: ({x,y} * 2 + q) * L + lane
-    uint4* scratch;          // ((e * 2 + {num,den}) * 2 + q) * L + lane, e < 2 half + 2
+    uint4* scratch;          // ((e * 2 + {num,den}) * 2 + q) * S + slot, e < 2 half + 2
+    uint32_t* work;          // next block of lanes to take, zero at launch
+    uint32_t slots_n;        // S: persistent CTAs x block, the scratch slots
     const uint32_t* bitmap;  // prefix bitmap as 32-bit words (nullptr: none)
     uint32_t bits;
     HitRec* hits;
@@ -145,7 +147,10 @@ struct MatchArgs {
 
 cudaError_t launch_init(const InitArgs& a, int block, cudaStream_t s);
 cudaError_t launch_match(const MatchArgs& a, int grid, cudaStream_t s);
-cudaError_t launch_paired(const PairedArgs& a, int block, cudaStream_t s);
+// The paired kernel is persistent: `grid` CTAs (the resident ones) take the
+// lanes a block at a time from `work`, so the scratch covers only the lanes
+// in flight and no SM idles in a tail wave.
+cudaError_t launch_paired(const PairedArgs& a, int block, int grid, cudaStream_t s);
 cudaError_t launch_chain(const ChainArgs& a, int block, cudaStream_t s);
 
 // Register and shared-memory footprint of the search kernels, for the shape

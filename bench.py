@@ -253,7 +253,10 @@ def batched_leg(dev, shape, cap):
 
     all_searches = workloads.config4_searches()
     searches = [s for s in all_searches if s.expected_candidates() <= cap]
-    cfg = N.EngineConfig(N.SCHEME_PAIRED, SHORT_HALF, 0, 0, 128, 0, 0)
+    # one search at a time, as the run driver does: half 256 and one lane per
+    # thread of two waves of resident blocks (1.2e8 candidates an advance), so
+    # that a small search does not overshoot its quota by much
+    cfg = N.EngineConfig(N.SCHEME_PAIRED, SHORT_HALF, 2 * dev.sms * 6 * 128, 0, 128, 0, 0)
     t0 = time.perf_counter()
     plain, plain_examined, plain_launches = {}, 0, 0
     for s in searches:
@@ -562,6 +565,7 @@ def main():
     # serves the whole run: it is created (host precompute, H2D of the start
     # point, tables and bitmap) and freed inside the timed region, and every
     # step is `advances` advances with the D2H of their survivors.
+    eng.close()  # the plain line's engine is done; the e2e run makes its own
     e2e = None
     if not args.no_e2e:
         h2d = d2h = 0

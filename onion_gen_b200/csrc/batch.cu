@@ -104,7 +104,7 @@ struct BatchArgs {
     Counters* counters;
     uint32_t nblocks;
     uint4* lanes;  // ({x,y} * 2 + q) * slots + slot
-    uint4* scratch;
+    uint4* scratch;  // per persistent CTA thread: ((e * 2 + w) * 2 + q) * grid * BLOCK + cta slot
     size_t slots;
     const uint4* table;
     const uint4* pow2;
@@ -157,7 +157,8 @@ __global__ void __launch_bounds__(OG_LB_THREADS, OG_LB_MIN_BLOCKS) batch_search_
         fe x = load_fe(a.lanes + 0 * a.slots + slot, a.slots);
         fe y = load_fe(a.lanes + 2 * a.slots + slot, a.slots);
         paired_rounds(x, y, words_fe(d.wx), words_fe(d.wy), words_fe(d.wt), qtab, a.half, a.rounds,
-                      a.scratch + slot, a.slots, [&](const fe& v, uint32_t step) { test_emit(sink, v, slot, step); });
+                      a.scratch + (blockIdx.x * BLOCK + threadIdx.x), (size_t)gridDim.x * BLOCK,
+                      [&](const fe& v, uint32_t step) { test_emit(sink, v, slot, step); });
         store_fe(a.lanes + 0 * a.slots + slot, a.slots, x);
         store_fe(a.lanes + 2 * a.slots + slot, a.slots, y);
     }
@@ -443,7 +444,9 @@ int og_batch_new(int ordinal, const og_batch_config* cfgp, og_batch** out, char*
     CU(cudaEventCreate(&b->ev1));
     const size_t S = cfg.slots;
     CU(b->lanes.alloc(S * 4));
-    CU(b->scratch.alloc(S * (2 * (size_t)cfg.half + 2) * 4));
+    // the scratch of the persistent CTAs, not of every slot: a CTA uses it for
+    // one block of slots at a time
+    CU(b->scratch.alloc((size_t)b->grid * BLOCK * (2 * (size_t)cfg.half + 2) * 4));
     const std::vector<uint4>& tab = pair_table(cfg.half);
     CU(b->table.alloc(tab.size()));
     CU(cudaMemcpyAsync(b->table.p, tab.data(), tab.size() * sizeof(uint4), cudaMemcpyHostToDevice, b->stream));

@@ -2,9 +2,12 @@
 //
 // Mirrors cuda::Engine (src/gpu/cuda.rs:103-365) and the shape logic of
 // gpu::Engine (src/gpu/mod.rs:292-477): host precompute once, lane state
-// resident in HBM, one kernel launch per advance, one synchronisation, a
-// copy of only the survivors that were written, and an overflow that is an
-// error rather than a truncation.
+// resident in HBM, one persistent kernel launch per advance, a copy of only
+// the survivors that were written, and an overflow that is an error rather
+// than a truncation. Two advances can be in flight, each with its own record
+// buffers, so that one advance's survivors cross back and are checked while
+// the next one runs. The device match (og_engine_match_on_device, and the
+// filter engine of og_engine_new_filters) adds one kernel per advance.
 #include <cuda_runtime.h>
 
 #include <algorithm>

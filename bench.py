@@ -367,17 +367,18 @@ def pp_per_candidate(half):
 
 def small_case(args):
     """Three advances of one round each: the case the ncu summaries under
-    profiles/ are captured on. Half 256 (or --half) and one resident wave of
-    lanes (SMs x 6 blocks x 128) keep the scratch near 3.8 GB; the kernel is
-    the production one, and its DRAM bytes per candidate do not depend on the
-    shape (64 B written and read back per candidate)."""
+    profiles/ are captured on. Half 256 (or --half) keeps the scratch of the
+    persistent CTAs near 3.8 GB; the lanes are eight blocks per resident CTA
+    (SMs x 6 x 128 x 8), as in production. The kernel is the production one,
+    and its DRAM bytes per candidate do not depend on the shape (64 B written
+    and read back per candidate)."""
     from onion_gen_b200 import _native as N
     from onion_gen_b200 import filter as F
     from onion_gen_b200 import gpu, key, workloads
 
     dev = gpu.look()[0]
     half = args.half or 256
-    lanes = dev.sms * 6 * 128
+    lanes = dev.sms * 6 * 128 * 8
     fs = F.FilterSet.parse_all([workloads.config2_prefix()])
     words, bits = fs.index_words()
     start = key.start_point(workloads.seed(0))

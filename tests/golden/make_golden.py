@@ -132,6 +132,16 @@ def main(ref_root):
         json.dump(out, f, indent=1)
     print(f"wrote {len(keys)} keys, {len(offsets)} offsets, {len(field)} field cases")
 
+    # ---- config 1: a sample of its 2^20 candidates, by the verifier ----
+    # candidate i of the base scalar of seed LE32(0) is the key of scalar + 8 i
+    srng = random.Random(1)
+    idx = sorted(srng.sample(range(1 << 20), 1024))
+    pubs = [V.public_from_secret((base + 8 * i).to_bytes(32, "little")).hex() for i in idx]
+    with open(os.path.join(HERE, "config1_sample.json"), "w") as f:
+        json.dump({"generated_by": "tests/golden/make_golden.py", "seed": (0).to_bytes(32, "little").hex(),
+                   "index": idx, "public": pubs}, f)
+    print(f"wrote {len(idx)} config-1 keys")
+
 
 if __name__ == "__main__":
     main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -5,6 +5,7 @@ ctypes) and checks it against the oracle's restatement of the reference
 engines on the same seeded inputs: bit-exact keys, exact offsets, exact
 survivor sets.
 """
+import json
 import os
 
 import numpy as np
@@ -48,6 +49,12 @@ def test_chain_config1_bit_exact_against_batch_engine(oracle, device):
     want = np.frombuffer(oracle.chain_keys(start, 256, 1 << 20), dtype=np.uint8).reshape(-1, 32)
     bad = np.nonzero((keys != want).any(axis=1))[0]
     assert bad.size == 0, f"{bad.size} keys differ, first at offset {8 * int(bad[0])}"
+    # and 1024 of them against the reference's own verifier (tests/golden/config1_sample.json)
+    sample = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "config1_sample.json")))
+    for i, pub in zip(sample["index"], sample["public"]):
+        ref = bytearray(bytes.fromhex(pub))
+        ref[31] &= 0x7F
+        assert bytes(keys[i]) == bytes(ref), i
 
 
 def test_paired_bit_exact_two_rounds(oracle, device):

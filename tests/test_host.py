@@ -163,3 +163,16 @@ def test_match_many_agrees_with_match_key(native):
     got = fs.match_many(keys)
     want = [fs.match_key(bytes(k)) for k in keys]
     assert [(-1 if w is None else w) for w in want] == got.tolist()
+
+
+def test_rederivation_against_the_config1_sample(native):
+    """The host's independent re-derivation (offset -> secret -> public key)
+    gives the reference verifier's full keys, sign bit included, for 1024 of
+    config 1's candidates."""
+    sample = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "config1_sample.json")))
+    seed = B(sample["seed"])
+    for i, pub in zip(sample["index"], sample["public"]):
+        packed = bytearray(B(pub))
+        packed[31] &= 0x7F
+        pk, _ = native.key.check_hit(seed, 8 * i, bytes(packed))
+        assert pk.hex() == pub

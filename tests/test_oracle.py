@@ -172,3 +172,19 @@ def test_reference_hit_room(oracle):
     assert oracle.hit_room(0, 16) == 4096
     assert oracle.hit_room(1 << 40, 16) == 1 << 18
     assert oracle.hit_room(1 << 30, 20) == 4 * 1024 + 1024
+
+
+SAMPLE = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "config1_sample.json")))
+
+
+def test_config1_sample_against_reference_verifier(oracle):
+    """1024 of config 1's 2^20 candidates (seed LE32(0), candidate i = scalar
+    + 8 i), computed by the reference's own verifier: the oracle's chain
+    engine (src/batch.rs) gives the same keys, sign bit cleared."""
+    seed = bytes.fromhex(SAMPLE["seed"])
+    start = oracle.scalar_base_mult(oracle.secret_scalar(seed))
+    keys = oracle.chain_keys_mt(start, 0, 1 << 20)
+    for i, pub in zip(SAMPLE["index"], SAMPLE["public"]):
+        want = bytearray(bytes.fromhex(pub))
+        want[31] &= 0x7F
+        assert keys[32 * i: 32 * i + 32] == bytes(want), i

@@ -142,13 +142,20 @@ def test_paired_bitmap_survivors_equal_oracle(oracle, device):
 
 
 def test_paired_wide_bitmap_many_prefixes(oracle, device):
-    """Config 3's shape on a 2^22 sub-range: 10,000 prefixes of 3..8 symbols,
-    24-bit index at ~5% occupancy."""
+    """Config 3 on its parity sub-range: 10,000 prefixes of 3..8 symbols, a
+    24-bit index at ~5% occupancy, the first 16.8 M candidates (2^24 and a
+    little more): the same ~840 k survivors as the oracle's, and the same
+    exact matches."""
     prefixes = workloads.config3_prefixes()
-    start, fs, got = filtered_parity(oracle, device, prefixes, 0, 128, 1024, 16, 0)
-    assert fs.bits == 24
-    for off, packed in got[:200]:
-        key.check_hit(workloads.seed(0), off, packed)
+    start, fs, got = filtered_parity(oracle, device, prefixes, 0, 128, 4096, 16, 0)
+    assert fs.bits == 24 and len(got) > 700_000
+    packed = np.frombuffer(b"".join(p for _, p in got), dtype=np.uint8).reshape(-1, 32)
+    ofs = oracle.FilterSet(prefixes)
+    m = fs.match_many(packed)
+    for k in range(0, len(got), 97):
+        assert m[k] == ofs.match(got[k][1])
+    for off, p in got[:200]:
+        key.check_hit(workloads.seed(0), off, p)
 
 
 def test_overflow_is_an_error_not_a_truncation(oracle, device):

@@ -82,9 +82,10 @@ class Batch:
 
     def results(self, search_id: int):
         st = self.status(search_id)
-        buf = (N.BatchHit * max(1, st.quota))()
+        room = max(1, min(st.quota, st.hits))
+        buf = (N.BatchHit * room)()
         n = C.c_size_t()
-        rc = N.lib.og_batch_results(self._h, search_id, buf, st.quota, C.byref(n))
+        rc = N.lib.og_batch_results(self._h, search_id, buf, room, C.byref(n))
         if rc:
             raise N.OgError(rc, f"search {search_id}")
         return [_hit(buf[i]) for i in range(n.value)]

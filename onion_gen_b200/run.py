@@ -83,3 +83,37 @@ def device_search(device, seed: bytes, prefixes, quota: int, threads: int = 0, c
         eng.close()
     found.sort(key=lambda h: h.offset)
     return found[:quota], examined, advances
+
+
+UNLIMITED = 0xFFFFFFFF
+
+
+def search_lease(device, root: bytes, first_block: int, blocks: int, filters, report, keep_going=None,
+                 max_steps=None, **batch_shape):
+    """A worker's leased range (worker::search, src/worker/run.rs:167-238) on
+    one GPU: blocks first_block .. first_block + blocks - 1 of `root`, each
+    searched from its own seed (block_seed, src/run.rs:211-221), all of them
+    at once in the batched engine, until `keep_going()` says stop or
+    `max_steps` steps have run.
+
+    Every find is handed to ``report(block, offset)`` as soon as its step
+    ends, already confirmed and re-derived on the host: positions are what
+    cross the wire, as in the reference. Within a block, finds come in offset
+    order. ``report`` returns whether to go on (the reference's callback does
+    the same). Returns the number of steps run."""
+    from . import batch as B
+
+    b = B.Batch(device, max_searches=max(blocks, 1), **batch_shape)
+    try:
+        for blk in range(first_block, first_block + blocks):
+            b.admit(blk, key.block_seed(root, blk), filters, UNLIMITED)
+        steps = 0
+        while (keep_going is None or keep_going()) and (max_steps is None or steps < max_steps):
+            hits = b.step()
+            steps += 1
+            for h in hits:
+                if not report(h.search_id, h.offset):
+                    return steps
+        return steps
+    finally:
+        b.close()

@@ -199,3 +199,33 @@ def test_suffix_searches_in_a_batch_agree_with_the_single_engine(device):
             addr = key.address(h.public_key)
             assert addr.endswith(t[7:]) if t.startswith("suffix:") else addr.startswith(t)
     b.close()
+
+
+def test_a_leased_range_reports_every_block_s_finds_in_order(device):
+    """run.search_lease: three blocks of a root seed searched at once; each
+    find re-derives from its block's seed and matches a filter, and each
+    block's finds are the single engine's first hits of that block's seed."""
+    from onion_gen_b200 import filter as F
+    from onion_gen_b200 import key
+
+    root = bytes(range(32))
+    filters = ["ab", "q7"]
+    finds = {}
+
+    def report(block, offset):
+        finds.setdefault(block, []).append(offset)
+        return True
+
+    steps = run.search_lease(device, root, 400, 3, filters, report, max_steps=6, half=64, slots=128 * 64)
+    assert steps == 6 and sorted(finds) == [400, 401, 402]
+    fs = F.FilterSet.parse_all(filters)
+    cfg = N.EngineConfig(0, 64, 1024, 2, 128, 0, 0)
+    for blk, offs in finds.items():
+        assert offs == sorted(offs)
+        seed = key.block_seed(root, blk)
+        for off in offs[:20]:
+            secret = key.expanded_secret_at_offset(seed, off)
+            pk = key.pack(key.scalar_base_mult(secret[:32]))
+            assert fs.match_address(pk) is not None
+        found, _, _ = run.device_search(device, seed, filters, len(offs), config=cfg)
+        assert [h.offset for h in found] == offs

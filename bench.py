@@ -258,14 +258,14 @@ def batched_leg(dev, shape, cap):
     """Config 4: plain (one engine per search) against batched, same searches."""
     from onion_gen_b200 import _native as N
     from onion_gen_b200 import batch as B
-    from onion_gen_b200 import run, workloads
+    from onion_gen_b200 import gpu, run, workloads
 
     all_searches = workloads.config4_searches()
     searches = [s for s in all_searches if s.expected_candidates() <= cap]
     # one search at a time, as the run driver does: half 256 and one lane per
     # thread of two waves of resident blocks (1.2e8 candidates an advance), so
     # that a small search does not overshoot its quota by much
-    cfg = N.EngineConfig(N.SCHEME_PAIRED, SHORT_HALF, 2 * dev.sms * 6 * 128, 0, 128, 0, 0)
+    cfg = N.EngineConfig(N.SCHEME_PAIRED, SHORT_HALF, 2 * gpu.resident_lanes(dev), 0, 128, 0, 0)
     t0 = time.perf_counter()
     plain, plain_examined, plain_launches = {}, 0, 0
     for s in searches:
@@ -369,7 +369,7 @@ def small_case(args):
     """Three advances of one round each: the case the ncu summaries under
     profiles/ are captured on. Half 256 (or --half) keeps the scratch of the
     persistent CTAs near 3.8 GB; the lanes are eight blocks per resident CTA
-    (SMs x 6 x 128 x 8), as in production. The kernel is the production one,
+    (SMs x 5 x 128 x 8), as in production. The kernel is the production one,
     and its DRAM bytes per candidate do not depend on the shape (64 B written
     and read back per candidate)."""
     from onion_gen_b200 import _native as N
@@ -378,7 +378,7 @@ def small_case(args):
 
     dev = gpu.look()[0]
     half = args.half or 256
-    lanes = dev.sms * 6 * 128 * 8
+    lanes = gpu.resident_lanes(dev) * 8
     fs = F.FilterSet.parse_all([workloads.config2_prefix()])
     words, bits = fs.index_words()
     start = key.start_point(workloads.seed(0))
@@ -401,7 +401,7 @@ def suffix_small_case(args):
     dev = gpu.look()[0]
     fs = F.FilterSet.parse_all(workloads.suffix_filters(40, 8))
     start = key.start_point(workloads.seed(0))
-    lanes = dev.sms * 6 * 128
+    lanes = gpu.resident_lanes(dev)
     eng = gpu.Engine(dev, start, filters=fs, config=N.EngineConfig(0, args.half or 256, lanes, 1, 128, 0, 0))
     for i in range(3):
         o, _, _ = eng.advance_matches_raw()

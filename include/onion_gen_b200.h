@@ -106,6 +106,11 @@ uint64_t og_engine_batch(const og_engine* e);
 size_t og_engine_room(const og_engine* e);
 /* The shape in use. */
 void og_engine_shape(const og_engine* e, og_engine_config* cfg);
+/* Lanes one wave of the search kernel of `scheme` holds on device `ordinal`:
+ * resident blocks per SM x SMs x `block` (0: 128). The paired kernel runs
+ * exactly this many threads and they take the lanes a block at a time. */
+int og_engine_resident_lanes(int ordinal, uint32_t scheme, uint32_t block, uint32_t* lanes, char* err,
+                             size_t errlen);
 
 /* Engine::advance (src/gpu/mod.rs:470, src/gpu/cuda.rs:282-365): moves every
  * lane on by one launch and writes each survivor to `out` (room `cap`),

@@ -148,6 +148,7 @@ def _load():
     sig("og_engine_batch", U64, [P])
     sig("og_engine_room", SZ, [P])
     sig("og_engine_shape", None, [P, C.POINTER(EngineConfig)])
+    sig("og_engine_resident_lanes", I, [I, U32, U32, C.POINTER(U32), B, SZ])
     sig("og_engine_advance", I, [P, P, SZ, C.POINTER(SZ), B, SZ])
     sig("og_engine_launch", I, [P, B, SZ])
     sig("og_engine_collect", I, [P, P, SZ, C.POINTER(SZ), B, SZ])

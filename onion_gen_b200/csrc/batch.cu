@@ -40,7 +40,7 @@
 #define OG_LB_THREADS 128
 #endif
 #ifndef OG_LB_MIN_BLOCKS
-#define OG_LB_MIN_BLOCKS 6
+#define OG_LB_MIN_BLOCKS 5
 #endif
 
 namespace og {

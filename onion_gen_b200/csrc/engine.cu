@@ -638,6 +638,18 @@ int og_device_info(int ordinal, char* name, size_t namelen, uint64_t* memory, in
     return OG_OK;
 }
 
+int og_engine_resident_lanes(int ordinal, uint32_t scheme, uint32_t block, uint32_t* lanes, char* err,
+                             size_t errlen) {
+    if (!lanes) return fail(err, errlen, OG_E_ARG, "null argument");
+    if (scheme != OG_SCHEME_PAIRED && scheme != OG_SCHEME_CHAIN)
+        return fail(err, errlen, OG_E_ARG, "unknown scheme %u", scheme);
+    if (block == 0) block = 128;
+    if (block % 32 != 0 || block > 1024) return fail(err, errlen, OG_E_ARG, "block %u: a multiple of 32 up to 1024", block);
+    cudaError_t e = cudaSetDevice(ordinal);
+    if (e != cudaSuccess) return fail(err, errlen, OG_E_DEVICE, "device %d: %s", ordinal, cuda_text(e).c_str());
+    return resident_lanes(ordinal, scheme, 0, block, lanes, err, errlen);
+}
+
 int og_engine_new_config(int ordinal, const uint8_t start[128], const og_engine_config* cfg, const uint64_t* bitmap,
                          size_t words, uint32_t bits, og_engine** out, char* err, size_t errlen) {
     og_engine_config c{};

@@ -1,14 +1,16 @@
 """Generates field_asm.cuh: GF(2^255-19) multiply and square for sm_100a.
 
 Eight 32-bit limbs, least significant first; inputs and outputs below 2^256
-(not canonical). The 512-bit product is accumulated by product scanning in
-64-bit slots: every partial product a_i*b_j is added as one 64-bit quantity
-(its low half then its high half, back to back in one PTX carry chain), so
-the pair maps to one wide multiply-add. Row i runs two chains: products whose
-position i+j is even (slots (i,i+1), (i+2,i+3), ...), then the odd ones. The
-accumulated value after each chain is below 2^(32*(i+9)), which is what lets
-the carry out of word i+8 be dropped and a fresh word take a bare carry.
-The 512-bit result is folded with 2^256 = 38 (mod 2^255-19) the same way.
+(not canonical). The 512-bit product is accumulated by operand scanning in 64-bit slots:
+every partial product a_i*b_j is added as one 64-bit quantity (its low half
+then its high half, back to back in one PTX carry chain), so the pair maps
+to one wide multiply-add. Slots at even positions i+j go to one accumulator
+and slots at odd positions to another, merged by one add chain at the end:
+with a single accumulator a word is the high half of one slot and the low
+half of the next, and the misaligned register pairs cost extra instructions
+on the multiply pipe (on B200: 0.387 multiplications/clk/SM with one
+accumulator, 0.411 with two). The 512-bit result is folded with
+2^256 = 38 (mod 2^255-19) the same way.
 (A one-level Karatsuba variant, 48 wide products plus carry corrections on
 the ALU, measured no faster on sm_100a: the ALU work it adds cancels the
 multiply-pipe work it saves.)
@@ -57,43 +59,69 @@ class Emit:
             self.live[carry_to] = True
 
 
+def merge(E, O, L):
+    """E += O over words 1..15 (the sum is below 2^512: no carry out)."""
+    first = True
+    for k in range(1, 16):
+        dst = f"t{k}"
+        src = dst if E.live[k] else "0"
+        if O.live[k]:
+            L.append(("add.cc.u32" if first else "addc.cc.u32") + f" {dst}, {src}, o{k};")
+            first = False
+        elif not first:
+            L.append(f"addc.cc.u32 {dst}, {src}, 0;")
+        else:
+            continue
+        E.live[k] = True
+    L[-1] = L[-1].replace("addc.cc.u32", "addc.u32")
+
+
 def mul_body(A, Bv):
-    e = Emit("t")
+    """Row i adds a_i * b into two accumulators: E takes the 64-bit slots at
+    even positions i + j, O those at odd positions. Each accumulator only
+    ever sees slots of one alignment, so every slot is an aligned register
+    pair. Of a row's two chains, the one whose last slot ends at word i + 7
+    carries into word i + 8; the other ends at word i + 8 and its carry is
+    zero (each accumulator holds a subset of rows 0..i, below 2^(32*(i+9)))."""
+    E, O = Emit("t"), Emit("o")
+    O.lines = E.lines
     for i in range(8):
-        even = [(i + j, A(i), Bv(j)) for j in range(0, 8, 2)]
-        odd = [(i + j, A(i), Bv(j)) for j in range(1, 8, 2)]
-        e.chain(even, carry_to=i + 8)
-        e.chain(odd, carry_to=None)
-    return e.lines
+        j0 = i % 2  # j with i + j even
+        ev = [(i + j, A(i), Bv(j)) for j in range(j0, 8, 2)]
+        od = [(i + j, A(i), Bv(j)) for j in range(1 - j0, 8, 2)]
+        E.chain(ev, carry_to=i + 8 if j0 == 0 else None)
+        O.chain(od, carry_to=i + 8 if j0 == 1 else None)
+    merge(E, O, E.lines)
+    return E.lines
 
 
 def sq_body(A):
-    e = Emit("t")
-    # off-diagonal products a_i a_j, i < j, at position i + j
+    """Off-diagonal products a_i a_j (i < j) at odd positions into O, at even
+    positions into E; then E += O, doubled, plus the squares a_i^2 (even
+    positions, into E)."""
+    E, O = Emit("t"), Emit("o")
+    O.lines = E.lines
     for i in range(7):
         js = list(range(i + 1, 8))
-        even = [(i + j, A(i), A(j)) for j in js if (j - (i + 1)) % 2 == 0]
-        odd = [(i + j, A(i), A(j)) for j in js if (j - (i + 1)) % 2 == 1]
-        top = i + 8 if i + 8 <= 15 else None
-        if even:
-            last_even_hi = even[-1][0] + 1
-            e.chain(even, carry_to=last_even_hi + 1 if last_even_hi + 1 <= 15 else None)
-        if odd:
-            last_odd_hi = odd[-1][0] + 1
-            e.chain(odd, carry_to=last_odd_hi + 1 if last_odd_hi + 1 <= 15 else None)
-    L = e.lines
-    # double t1..t14 (t0 is still empty), carry into t15
+        for acc, par in ((O, 1), (E, 0)):
+            prods = [(i + j, A(i), A(j)) for j in js if (i + j) % 2 == par]
+            if prods:
+                c = prods[-1][0] + 2
+                acc.chain(prods, carry_to=c if c <= 15 else None)
+    L = E.lines
+    merge(E, O, L)
     for k in range(16):
-        if not e.live[k]:
+        if not E.live[k]:
             L.append(f"mov.u32 t{k}, 0;")
-            e.live[k] = True
+            E.live[k] = True
+    # double t1..t15 (t0 is still empty; the doubled sum is below 2^512)
     L.append("add.cc.u32 t1, t1, t1;")
     for k in range(2, 15):
         L.append(f"addc.cc.u32 t{k}, t{k}, t{k};")
     L.append("addc.u32 t15, t15, t15;")
     # diagonal squares a_i^2 at position 2i: one chain of 64-bit slots
     diag = [(2 * i, A(i), A(i)) for i in range(8)]
-    e.chain(diag, carry_to=None)
+    E.chain(diag, carry_to=None)
     return L
 
 
@@ -133,7 +161,7 @@ def emit_fn(name, body, nin, extra=""):
         else "const uint32_t* __restrict__ a"
     )
     out.append(f"__device__ __forceinline__ void {name}(uint32_t* __restrict__ r, {sig}) {{")
-    out.append('    asm("{\\n\\t.reg .u32 t<17>;\\n\\t.reg .u32 r<9>;\\n\\t' + extra + '"')
+    out.append('    asm("{\\n\\t.reg .u32 t<17>;\\n\\t.reg .u32 o<17>;\\n\\t.reg .u32 r<9>;\\n\\t' + extra + '"')
     for line in body + reduce_tail():
         out.append(f'        "{line}\\n\\t"')
     out.append('        "}"')

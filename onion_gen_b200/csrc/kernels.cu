@@ -6,14 +6,15 @@
 #include "suffix_match.cuh"
 
 // Register budget of the search kernels: at most OG_LB_THREADS threads per
-// block and at least OG_LB_MIN_BLOCKS resident blocks per SM. 128 x 6 caps
-// them at 80 registers (24 warps per SM), measured fastest on B200 against
-// 96 (20 warps), 128 (16) and 130 registers.
+// block and at least OG_LB_MIN_BLOCKS resident blocks per SM. 128 x 5 caps
+// them at 96 registers (20 warps per SM). With the two-accumulator field
+// multiply this measured fastest on B200: 20.5 G keys/s against 20.0 at
+// 80 registers (24 warps, more spills) and 20.3 at 128 (16 warps).
 #ifndef OG_LB_THREADS
 #define OG_LB_THREADS 128
 #endif
 #ifndef OG_LB_MIN_BLOCKS
-#define OG_LB_MIN_BLOCKS 6
+#define OG_LB_MIN_BLOCKS 5
 #endif
 
 namespace og {

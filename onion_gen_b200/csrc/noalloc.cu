@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(NBLOCK) noalloc_init_kernel(const NoAllocArgs 
 
 // The production paired kernel with its scratch in the file-scope array; the
 // table is read through L1 as in the single engine.
-__global__ void __launch_bounds__(NBLOCK, 6) noalloc_paired_kernel(const NoAllocArgs a) {
+__global__ void __launch_bounds__(NBLOCK, 5) noalloc_paired_kernel(const NoAllocArgs a) {
     const uint4* qtab = a.table;
     const uint32_t lane = blockIdx.x * blockDim.x + threadIdx.x;
     const size_t L = a.lanes_n;

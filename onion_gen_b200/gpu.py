@@ -54,6 +54,17 @@ def look():
     return out
 
 
+def resident_lanes(device, scheme=None, block=128):
+    """Lanes one wave of the search kernel holds on ``device``: resident
+    blocks per SM x SMs x ``block``. The paired kernel runs exactly this
+    many threads; its lanes are taken a block at a time."""
+    n = C.c_uint32()
+    err = N.errbuf()
+    scheme = N.SCHEME_PAIRED if scheme is None else scheme
+    N.check(N.lib.og_engine_resident_lanes(device.ordinal, scheme, block, C.byref(n), err, 512), err)
+    return n.value
+
+
 def _words(bitmap):
     if bitmap is None:
         return None, 0

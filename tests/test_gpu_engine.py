@@ -217,3 +217,22 @@ def test_bitmap_width_extremes(oracle, device, bits):
     prefixes = ["abc", "q7x"]
     start, fs, got = filtered_parity(oracle, device, prefixes, bits, 64, 1024, 4, 4)
     assert fs.bits == bits and len(got) > 0
+
+
+def test_default_shape_is_eight_blocks_per_resident_cta(oracle, device):
+    """og_engine_resident_lanes reports one wave of the paired kernel; an
+    engine built with lanes 0 takes eight blocks of 128 per resident CTA and
+    half 2048, and its first advance tiles the range."""
+    resident = gpu.resident_lanes(device)
+    assert resident % (128 * device.sms) == 0 and resident >= 128 * device.sms
+    start = oracle_start(oracle, workloads.seed(2))
+    fs = F.FilterSet.parse_all(["abcdefg"])
+    words, bits = fs.index_words()
+    eng = gpu.Engine(device, start, bitmap=words, bitmap_bits=bits, config=cfg(N.SCHEME_PAIRED, 0, 0, 1, dump=0))
+    shape = eng.shape()
+    assert shape.half == 2048 and eng.threads() == 8 * resident
+    assert eng.batch() == 8 * resident * (2 * 2048 + 1)
+    for s in eng.advance()[:20]:
+        key.check_hit(workloads.seed(2), s.offset, s.packed)
+    with pytest.raises(N.OgError):
+        gpu.resident_lanes(device, scheme=7)

@@ -236,3 +236,31 @@ def test_default_shape_is_eight_blocks_per_resident_cta(oracle, device):
         key.check_hit(workloads.seed(2), s.offset, s.packed)
     with pytest.raises(N.OgError):
         gpu.resident_lanes(device, scheme=7)
+
+
+def test_reference_gpu_harness_case(device):
+    """The reference's own device check (benches/gpu-chain.rs:15-94): filter
+    "abc", seed [7; 32], 2^14 threads, four launches through the
+    reference-shaped constructor. Every survivor is re-derived from its
+    offset alone and must equal the device's key (sign bit masked); the
+    index must let something through; an exact match spells "abc"."""
+    seed = bytes([7] * 32)
+    fs = F.FilterSet.parse_all(["abc"])
+    words, bits = fs.index_words()
+    eng = gpu.Engine(device, key.start_point(seed), threads=1 << 14, bitmap=words, bitmap_bits=bits)
+    assert eng.threads() == 1 << 14
+    examined, offsets, confirmed = 0, set(), 0
+    for _ in range(4):
+        hits = eng.advance()
+        examined += eng.batch()
+        for h in hits:
+            pk, _ = key.check_hit(seed, h.offset, h.packed)
+            assert pk[:31] == h.packed[:31] and (pk[31] & 0x7F) == h.packed[31]
+            assert h.offset % 8 == 0 and 0 < h.offset <= 8 * examined and h.offset not in offsets
+            offsets.add(h.offset)
+            if fs.match_key(h.packed) is not None:
+                confirmed += 1
+                assert key.address(pk).startswith("abc")
+    assert examined == 4 * eng.batch() and len(offsets) > 0
+    # a 15-bit literal on its index: about examined / 2^15 exact matches
+    assert 0.5 * examined / 2**15 < confirmed < 1.5 * examined / 2**15

@@ -9,7 +9,9 @@
 // block and at least OG_LB_MIN_BLOCKS resident blocks per SM. 128 x 5 caps
 // them at 96 registers (20 warps per SM). With the two-accumulator field
 // multiply this measured fastest on B200: 20.5 G keys/s against 20.0 at
-// 80 registers (24 warps, more spills) and 20.3 at 128 (16 warps).
+// 80 registers (24 warps, more spills) and 20.3 at 128 (16 warps). With the
+// lane's centre parked in shared memory (paired_rounds) it spills 4 bytes
+// and runs 20.8; at 80 registers 20.9 at half 2048 but 20.7 at half 1024.
 #ifndef OG_LB_THREADS
 #define OG_LB_THREADS 128
 #endif

@@ -29,6 +29,7 @@ namespace {
 
 constexpr size_t SCRATCH_BYTES = OG_NOALLOC_SCRATCH_BYTES;
 constexpr uint32_t NBLOCK = 128;
+static_assert(NBLOCK <= PARK_STRIDE, "paired_rounds parks PARK_STRIDE lanes per block");
 constexpr uint32_t POW2 = 24;
 constexpr int MAX_DEVICES = 64;
 

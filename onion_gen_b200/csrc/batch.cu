@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(OG_LB_THREADS, OG_LB_MIN_BLOCKS) batch_search_
         const Sink sink{d.bitmap, d.bits, a.surv, &a.counters->surv, a.surv_cap, sb.sidx, d.sbitmap, d.sbits};
         fe x = load_fe(a.lanes + 0 * a.slots + slot, a.slots);
         fe y = load_fe(a.lanes + 2 * a.slots + slot, a.slots);
-        paired_rounds(x, y, words_fe(d.wx), words_fe(d.wy), words_fe(d.wt), qtab, a.half, a.rounds,
+        paired_rounds<false>(x, y, words_fe(d.wx), words_fe(d.wy), words_fe(d.wt), qtab, a.half, a.rounds,
                       a.scratch + (blockIdx.x * BLOCK + threadIdx.x), (size_t)gridDim.x * BLOCK,
                       [&](const fe& v, uint32_t step) { test_emit(sink, v, slot, step); });
         store_fe(a.lanes + 0 * a.slots + slot, a.slots, x);

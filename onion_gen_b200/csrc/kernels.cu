@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(OG_LB_THREADS, OG_LB_MIN_BLOCKS) paired_kernel
         const uint32_t lane = item * blockDim.x + threadIdx.x;
         fe x = load_fe(a.lanes + 0 * L + lane, L);
         fe y = load_fe(a.lanes + 2 * L + lane, L);
-        paired_rounds(x, y, words_fe(a.wx), words_fe(a.wy), words_fe(a.wt), qtab, a.half, a.rounds, a.scratch + slot, S,
+        paired_rounds<true>(x, y, words_fe(a.wx), words_fe(a.wy), words_fe(a.wt), qtab, a.half, a.rounds, a.scratch + slot, S,
                       [&](const fe& v, uint32_t step) { test_emit(sink, v, lane, step); });
         store_fe(a.lanes + 0 * L + lane, L, x);
         store_fe(a.lanes + 2 * L + lane, L, y);

@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(NBLOCK, 5) noalloc_paired_kernel(const NoAlloc
     const Sink sink{a.bitmap, a.bits, a.hits, a.counter, a.cap, 0, nullptr, 0};
     fe x = load_fe(a.lanes + 0 * L + lane, L);
     fe y = load_fe(a.lanes + 2 * L + lane, L);
-    paired_rounds(x, y, words_fe(a.wx), words_fe(a.wy), words_fe(a.wt), qtab, a.half, a.rounds, a.scratch + lane, L,
+    paired_rounds<true>(x, y, words_fe(a.wx), words_fe(a.wy), words_fe(a.wt), qtab, a.half, a.rounds, a.scratch + lane, L,
                   [&](const fe& v, uint32_t step) { test_emit(sink, v, lane, step); });
 }
 

@@ -154,18 +154,16 @@ __device__ __forceinline__ void add_cached(fe& X, fe& Y, fe& Z, fe& T, const fe&
     T = fe_mulv(x3, y3);
 }
 
-// One lane's `rounds` paired rounds around its affine centre (x, y); see
-// kernels.cuh for the formulas and the candidate numbering. `scr` is the
-// lane's scratch: element e, part w (0 numerator, 1 denominator), half q at
-// scr + ((e * 2 + w) * 2 + q) * stride. `visit(y, step)` receives every
-// candidate's y (not yet canonical) with step = round * (2 half + 1) + index.
 // A lane's centre x, y and t = x y parked in shared memory for the forward
 // pass: each fe as two 16-byte quarters at park[(k * 2 + q) * PARK_STRIDE],
 // so a warp's loads are conflict-free. Loaded with volatile asm right
 // before each use so that the compiler cannot hoist them back into
 // registers for the whole loop. The 24 registers this frees took the
-// search kernel at 96 registers from 72 bytes of spills to 4 and from
-// 20.6 to 20.8 G keys/s on B200.
+// single-search kernel at 96 registers from 72 bytes of spills to 4 and
+// from 20.6 to 20.8 G keys/s on B200. The batched kernel does not park
+// (Park = false): the 12 KB of shared memory a block takes it from L1,
+// and that kernel, whose CTAs move between searches and their bitmaps,
+// ran 10 % slower parked.
 #ifndef OG_LB_THREADS
 #define OG_LB_THREADS 128  // the most threads a block of the search kernels has
 #endif
@@ -185,14 +183,20 @@ __device__ __forceinline__ fe unpark_fe(const uint4* park, int k) {
     return r;
 }
 
-template <class Visit>
+// One lane's `rounds` paired rounds around its affine centre (x, y); see
+// kernels.cuh for the formulas and the candidate numbering. `scr` is the
+// lane's scratch: element e, part w (0 numerator, 1 denominator), half q at
+// scr + ((e * 2 + w) * 2 + q) * stride. `visit(y, step)` receives every
+// candidate's y (not yet canonical) with step = round * (2 half + 1) + index.
+// Park: keep the centre in shared memory during the forward pass (above).
+template <bool Park, class Visit>
 __device__ __forceinline__ void paired_rounds(fe& x, fe& y, const fe& wx, const fe& wy, const fe& wt,
                                               const uint4* qtab, uint32_t half, uint32_t rounds, uint4* scr,
                                               size_t stride, Visit&& visit) {
     const size_t L = stride;
     const uint32_t slots = 2 * half + 1;
-    __shared__ uint4 park_s[6 * PARK_STRIDE];
-    uint4* const park = park_s + threadIdx.x;
+    __shared__ uint4 park_s[Park ? 6 * PARK_STRIDE : 1];
+    uint4* const park = park_s + (Park ? threadIdx.x : 0);
 #define SCR(e, w) (scr + ((size_t)(e) * 4 + (w) * 2) * L)
     for (uint32_t r = 0; r < rounds; r++) {
         const fe t = fe_mulv(x, y);
@@ -207,27 +211,30 @@ __device__ __forceinline__ void paired_rounds(fe& x, fe& y, const fe& wx, const 
             store_fe(SCR(1, 1), L, den1);
             run = fe_mulv(den0, den1);
         }
-        park_fe(park, 0, x);
-        park_fe(park, 1, y);
-        park_fe(park, 2, t);
+        if (Park) {
+            park_fe(park, 0, x);
+            park_fe(park, 1, y);
+            park_fe(park, 2, t);
+        }
+        const auto centre = [&](int k) -> fe { return Park ? unpark_fe(park, k) : k == 0 ? x : k == 1 ? y : t; };
 #pragma unroll 1
         for (uint32_t m = 1; m <= half; m++) {
             const uint4* q = qtab + (size_t)(m - 1) * 6;
-            const fe A = fe_mulv(unpark_fe(park, 0), load_fe(q + 2, 1));
-            const fe B = fe_mulv(unpark_fe(park, 1), load_fe(q + 0, 1));
+            const fe A = fe_mulv(centre(0), load_fe(q + 2, 1));
+            const fe B = fe_mulv(centre(1), load_fe(q + 0, 1));
             const fe d0 = fe_sub(A, B);  // P + Q_m
             const fe qt = load_fe(q + 4, 1);
-            store_fe(SCR(2 * m, 0), L, fe_mulv(fe_sub(unpark_fe(park, 2), qt), run));
+            store_fe(SCR(2 * m, 0), L, fe_mulv(fe_sub(centre(2), qt), run));
             store_fe(SCR(2 * m, 1), L, d0);
             run = fe_mulv(run, d0);
             const fe d1 = fe_add(A, B);  // P - Q_m
-            store_fe(SCR(2 * m + 1, 0), L, fe_mulv(fe_add(unpark_fe(park, 2), qt), run));
+            store_fe(SCR(2 * m + 1, 0), L, fe_mulv(fe_add(centre(2), qt), run));
             store_fe(SCR(2 * m + 1, 1), L, d1);
             run = fe_mulv(run, d1);
         }
         fe acc = fe_invert(run);
         const uint32_t base_step = r * slots;
-        visit(unpark_fe(park, 1), base_step + half);
+        visit(centre(1), base_step + half);
 #pragma unroll 1
         for (uint32_t m = half; m >= 1; m--) {
             {

@@ -65,10 +65,10 @@ BATCH_STEP_CAP_MS = 8.0
 CPU_HALF = 4096  # PairEngine::new(8192) (src/run.rs:601, src/batch.rs:32)
 # DRAM bytes per candidate of paired_kernel, from one ncu capture of one
 # launch at the plain line's shape (half 2048, 757,760 lanes on 740 persistent
-# CTAs: dram__bytes_read.sum + dram__bytes_write.sum = 199.28 + 198.91 GB for
+# CTAs: dram__bytes_read.sum + dram__bytes_write.sum = 198.88 + 198.85 GB for
 # 3,104,542,720 candidates); the algorithmic figure is 128 B (the Montgomery
 # scratch, 64 B written and 64 B read per candidate) whatever the shape.
-TRAFFIC_PER_CANDIDATE = 128.26
+TRAFFIC_PER_CANDIDATE = 128.11
 ALGORITHMIC_BYTES_PER_CANDIDATE = 128
 
 

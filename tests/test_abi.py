@@ -45,6 +45,22 @@ def test_no_device_is_an_ordinary_outcome(native):
         assert native.gpu.look() == []
 
 
+def test_resident_lanes_checks_arguments_before_the_device(native):
+    """og_engine_resident_lanes refuses a bad scheme or block as OG_E_ARG
+    whether or not a device is present; without one it reports a status."""
+    n = ctypes.c_uint32(0)
+    err = native._native.errbuf()
+    L = native._native.lib
+    assert native._native.STATUS[L.og_engine_resident_lanes(0, 7, 128, ctypes.byref(n), err, 512)] == "OG_E_ARG"
+    assert native._native.STATUS[L.og_engine_resident_lanes(0, 0, 100, ctypes.byref(n), err, 512)] == "OG_E_ARG"
+    assert native._native.STATUS[L.og_engine_resident_lanes(0, 0, 128, None, err, 512)] == "OG_E_ARG"
+    rc = L.og_engine_resident_lanes(0, 0, 128, ctypes.byref(n), err, 512)
+    if native.gpu.look():
+        assert rc == 0 and n.value % 128 == 0 and n.value > 0
+    else:
+        assert rc != 0 and native._native.STATUS[rc] in ("OG_E_DEVICE", "OG_E_NODEVICE")
+
+
 def test_engine_without_device_reports_status(native, oracle):
     import pytest
 

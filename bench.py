@@ -171,16 +171,39 @@ class Clocks:
         }
 
 
+def plain_workload(prefix):
+    return "plain search: seed LE32(0), prefix %r (16-bit index), 2^32 candidates per step" % prefix
+
+
+def config2_search():
+    """Config 2's seed, prefix and prefix index for the CPU legs, without the
+    product's library: the workload generator loaded from its file and the
+    oracle's FilterSet."""
+    import importlib.util
+
+    from oracle import oracle as O
+
+    spec = importlib.util.spec_from_file_location("og_workloads", os.path.join(ROOT, "onion_gen_b200", "workloads.py"))
+    W = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = W
+    spec.loader.exec_module(W)
+    prefix = W.config2_prefix()
+    fs = O.FilterSet([prefix])
+    return W.seed(0), prefix, fs.words(), fs.bits
+
+
 def cpu_baseline(seconds):
     """The reference's paired CPU engine restated (oracle/), timed the way
     src/estimate.rs:86-117 does: one untimed round, then the median of three
-    timed runs on every host thread. The chain engine (src/batch.rs) is timed
-    beside it for context."""
+    timed runs on every host thread, each thread on its own sub-range of
+    config 2's search with config 2's prefix index. The chain engine
+    (src/batch.rs) is timed beside it for context."""
     from oracle import oracle as O
 
     threads = os.cpu_count() or 1
-    O.pair_rate(threads, 0.5, CPU_HALF)  # untimed round
-    runs = [O.pair_rate(threads, seconds / 3, CPU_HALF) for _ in range(3)]
+    seed, prefix, words, bits = config2_search()
+    O.pair_rate_search(threads, 0.5, CPU_HALF, seed, words, bits)  # untimed round
+    runs = [O.pair_rate_search(threads, seconds / 3, CPU_HALF, seed, words, bits) for _ in range(3)]
     rates = sorted(r for r, _ in runs)
     examined = sum(ex for _, ex in runs)
     chain, _ = O.chain_rate(threads, min(2.0, seconds / 3), 8192)
@@ -189,8 +212,9 @@ def cpu_baseline(seconds):
         "unit": "keys/s",
         "cores": threads,
         "kind": "port",
-        "sample": f"{examined} candidates of the paired CPU engine (batch 8192) with a 16-bit prefix probe: median of "
-        f"3 runs of {seconds / 3:.1f} s on {threads} threads after one untimed round",
+        "sample": f"{examined} candidates of config 2's search (seed LE32(0), prefix {prefix!r}, its {bits}-bit index) "
+        f"by the paired CPU engine (batch 8192), thread t from candidate 2^40 t: median of 3 runs of "
+        f"{seconds / 3:.1f} s on {threads} threads after one untimed round",
         "runs": rates,
         "chain_engine_keys_per_s": chain,
     }
@@ -204,11 +228,12 @@ def reference_arm(args):
 
     threads = os.cpu_count() or 1
     seconds = max(1.0, min(10.0, 60.0 / max(1, args.steps + args.warmup)))
+    seed, prefix, words, bits = config2_search()
     for _ in range(args.warmup):
-        O.pair_rate(threads, seconds, CPU_HALF)
+        O.pair_rate_search(threads, seconds, CPU_HALF, seed, words, bits)
     total, t = 0, 0.0
     for _ in range(args.steps):
-        r, ex = O.pair_rate(threads, seconds, CPU_HALF)
+        r, ex = O.pair_rate_search(threads, seconds, CPU_HALF, seed, words, bits)
         total += ex
         t += ex / r if r else 0
     value = total / t if t else 0.0
@@ -226,10 +251,11 @@ def reference_arm(args):
         "vs_baseline": None,
         "dtype": "u32",
         "data": "synthetic",
-        "config": {"workload": "config 2 shape on the host: paired CPU engine, seeds per thread, 16-bit prefix probe",
+        "config": {"workload": plain_workload(prefix), "engine": "paired CPU engine (batch 8192), restated in C",
                    "threads": threads},
         "cpu_baseline": {"value": value, "unit": "keys/s", "cores": threads, "kind": "port",
-                         "sample": f"{total} candidates, {args.steps} steps of {seconds:.1f} s on {threads} threads"},
+                         "sample": f"{total} candidates of the search, thread t from candidate 2^40 t: "
+                         f"{args.steps} steps of {seconds:.1f} s on {threads} threads"},
         "e2e": {"value": value, "unit": "keys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference's GPU engine is Rust->PTX built by a nightly toolchain absent here; its CPU engine "
         "is restated in C (oracle/) and timed instead",
@@ -632,7 +658,7 @@ def main():
             "dtype": "u32",
             "data": "synthetic",
             "config": {
-                "workload": "plain search: seed LE32(0), prefix %r (16-bit index), 2^32 candidates per step" % prefix,
+                "workload": plain_workload(prefix),
                 "scheme": "paired",
                 "half": shape.half,
                 "lanes": shape.lanes,

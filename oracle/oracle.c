@@ -996,6 +996,12 @@ typedef struct {
     uint64_t seed;
     uint64_t examined;
     double elapsed;
+    /* one search (orc_pair_rate_search): its seed, its index, the thread's
+     * place in it */
+    const uint8_t *search_seed;
+    const uint64_t *bitmap;
+    uint32_t bits;
+    int index;
 } rate_job;
 
 static double now_s(void) {
@@ -1009,16 +1015,29 @@ static void *rate_run(void *arg) {
     uint8_t seed[32] = {0};
     for (int i = 0; i < 8; i++) seed[i] = (uint8_t)(j->seed >> (8 * i));
     uint8_t sk[32];
-    orc_secret_scalar(seed, sk);
+    orc_secret_scalar(j->search_seed ? j->search_seed : seed, sk);
     point acc = scalar_base_mult(sk);
+    if (j->search_seed && j->index > 0) {
+        /* thread t starts 2^40 t candidates into the search */
+        const point off = multiple_of_eight_g((uint64_t)j->index << 40);
+        const cached c = to_cached(&off, two_d());
+        acc = add_p3(&acc, &c);
+    }
     if (j->which == 0) {
         pair_engine e;
         pair_new(&e, j->size);
-        /* a 16-bit index with one slot set, as a six-symbol prefix makes */
-        uint64_t *bm = calloc(1024, sizeof *bm);
-        bm[j->seed % 1024] = 1;
-        e.probe = bm;
-        e.probe_bits = 16;
+        /* a 16-bit index with one slot set, as a six-symbol prefix makes,
+         * unless the search's own index is given */
+        uint64_t *bm = NULL;
+        if (j->bitmap) {
+            e.probe = j->bitmap;
+            e.probe_bits = j->bits;
+        } else {
+            bm = calloc(1024, sizeof *bm);
+            bm[j->seed % 1024] = 1;
+            e.probe = bm;
+            e.probe_bits = 16;
+        }
         pair_begin(&e, &acc);
         pair_run(&e, &acc, NULL); /* untimed round */
         double t0 = now_s();
@@ -1052,7 +1071,8 @@ static void *rate_run(void *arg) {
     return NULL;
 }
 
-static double rate_common(int which, int threads, double seconds, size_t size, uint64_t *examined) {
+static double rate_common(int which, int threads, double seconds, size_t size, const uint8_t *search_seed,
+                          const uint64_t *bitmap, uint32_t bits, uint64_t *examined) {
     if (threads < 1) threads = 1;
     if (threads > 512) threads = 512;
     pthread_t *th = calloc(threads, sizeof *th);
@@ -1062,6 +1082,10 @@ static double rate_common(int which, int threads, double seconds, size_t size, u
         jobs[t].size = size;
         jobs[t].seconds = seconds;
         jobs[t].seed = 0x6f6e696f6e000000ULL + (uint64_t)t;
+        jobs[t].search_seed = search_seed;
+        jobs[t].bitmap = bitmap;
+        jobs[t].bits = bits;
+        jobs[t].index = t;
         pthread_create(&th[t], NULL, rate_run, &jobs[t]);
     }
     double rate = 0;
@@ -1078,11 +1102,20 @@ static double rate_common(int which, int threads, double seconds, size_t size, u
 }
 
 double orc_pair_rate(int threads, double seconds, size_t half, uint64_t *examined) {
-    return rate_common(0, threads, seconds, half, examined);
+    return rate_common(0, threads, seconds, half, NULL, NULL, 0, examined);
+}
+
+double orc_pair_rate_search(int threads, double seconds, size_t half, const uint8_t seed[32], const uint64_t *bitmap,
+                            uint32_t bits, uint64_t *examined) {
+    if (!seed || !bitmap || bits < 1 || bits > 32) {
+        if (examined) *examined = 0;
+        return 0;
+    }
+    return rate_common(0, threads, seconds, half, seed, bitmap, bits, examined);
 }
 
 double orc_chain_rate(int threads, double seconds, size_t batch, uint64_t *examined) {
-    return rate_common(1, threads, seconds, batch, examined);
+    return rate_common(1, threads, seconds, batch, NULL, NULL, 0, examined);
 }
 
 /* ========================================================================== */

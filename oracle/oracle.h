@@ -99,6 +99,11 @@ void orc_pair_keys(const uint8_t start[128], size_t half, size_t rounds,
  * from its own seed. Returns candidates per second; *examined receives the
  * total counted. */
 double orc_pair_rate(int threads, double seconds, size_t half, uint64_t *examined);
+/* The same on one search: the scalar of `seed`, thread t starting 2^40 t
+ * candidates into it (disjoint sub-ranges), every candidate probed in
+ * `bitmap` (top `bits` bits of the packed key, src/filter.rs:2538-2549). */
+double orc_pair_rate_search(int threads, double seconds, size_t half, const uint8_t seed[32], const uint64_t *bitmap,
+                            uint32_t bits, uint64_t *examined);
 /* Same for the chain engine (src/batch.rs). */
 double orc_chain_rate(int threads, double seconds, size_t batch, uint64_t *examined);
 

@@ -33,6 +33,9 @@ def lib():
         P, U8P, SZ, U64, U32 = C.c_void_p, C.c_char_p, C.c_size_t, C.c_uint64, C.c_uint32
         L.orc_pair_rate.restype = C.c_double
         L.orc_pair_rate.argtypes = [C.c_int, C.c_double, SZ, C.POINTER(U64)]
+        L.orc_pair_rate_search.restype = C.c_double
+        L.orc_pair_rate_search.argtypes = [C.c_int, C.c_double, SZ, C.c_char_p, C.c_void_p, C.c_uint32,
+                                           C.POINTER(U64)]
         L.orc_chain_rate.restype = C.c_double
         L.orc_chain_rate.argtypes = [C.c_int, C.c_double, SZ, C.POINTER(U64)]
         L.orc_fset_new.restype = P
@@ -268,6 +271,17 @@ def pair_keys(start: bytes, half: int, rounds: int):
 def pair_rate(threads: int, seconds: float, half: int = 96):
     ex = C.c_uint64()
     r = lib().orc_pair_rate(threads, seconds, half, C.byref(ex))
+    return r, ex.value
+
+
+def pair_rate_search(threads: int, seconds: float, half: int, seed: bytes, words, bits: int):
+    """pair_rate on one search: the seed's scalar, thread t 2^40 t candidates
+    into it, every candidate probed in the search's prefix index."""
+    import numpy as np
+
+    w = np.ascontiguousarray(np.asarray(words, dtype=np.uint64))
+    ex = C.c_uint64()
+    r = lib().orc_pair_rate_search(threads, seconds, half, bytes(seed), w.ctypes.data, bits, C.byref(ex))
     return r, ex.value
 
 

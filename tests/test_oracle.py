@@ -188,3 +188,13 @@ def test_config1_sample_against_reference_verifier(oracle):
         want = bytearray(bytes.fromhex(pub))
         want[31] &= 0x7F
         assert keys[32 * i: 32 * i + 32] == bytes(want), i
+
+
+def test_pair_rate_on_one_search(oracle):
+    """The CPU baseline's rate run over one search: a rate and a count for a
+    real prefix index; a missing index or a bad width is refused (0)."""
+    f = oracle.FilterSet(["cpejtg"])
+    r, ex = oracle.pair_rate_search(2, 0.2, 256, bytes(32), f.words(), f.bits)
+    assert r > 0 and ex > 0
+    r, ex = oracle.pair_rate_search(2, 0.2, 256, bytes(32), f.words(), 0)
+    assert r == 0 and ex == 0

@@ -210,10 +210,11 @@ def test_paired_pattern_bitmap_survivors_equal_oracle(oracle, device):
     assert len(got) > 100
 
 
-@pytest.mark.parametrize("bits", [8, 26])
+@pytest.mark.parametrize("bits", [8, 26, 32])
 def test_bitmap_width_extremes(oracle, device, bits):
-    """The narrowest index the engine takes and a 64 MiB one: the same
-    survivors as the oracle's."""
+    """The narrowest index the engine takes, a 64 MiB one and the widest
+    (32 bits, 512 MiB; the reference's --index-bits range is 8..32): the
+    same survivors as the oracle's."""
     prefixes = ["abc", "q7x"]
     start, fs, got = filtered_parity(oracle, device, prefixes, bits, 64, 1024, 4, 4)
     assert fs.bits == bits and len(got) > 0

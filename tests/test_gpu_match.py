@@ -181,3 +181,25 @@ def test_launch_and_collect_pipeline_equals_advance(device):
         assert all(np.array_equal(x[i], y[j]) for x, y in zip(w, g))
     assert sum(len(w[0]) for w in want) > 0
     d.close()
+
+
+@pytest.mark.parametrize("device_match", [False, True])
+def test_full_address_filters(device, device_match):
+    """Filters past the key-only symbols: a whole 56-symbol address and a
+    53-symbol prefix (sign bit and checksum symbols included), each built
+    from a key the first advance examines, and a whole address one symbol
+    off. The run driver finds exactly the two keys, confirmed on their
+    addresses, with the host match and with the device match."""
+    from onion_gen_b200 import run
+
+    seed = workloads.seed(9)
+    off1, off2 = 8 * (3 * SLOTS + 1 + 40), 8 * (700 * SLOTS + 1 + 200)
+    a1, a2 = key.address(key_at(seed, off1)), key.address(key_at(seed, off2))
+    decoy = a1[:30] + ("a" if a1[30] != "a" else "b") + a1[31:]
+    filters = [a1, a2[:53], decoy]
+    found, examined, advances = run.device_search(device, seed, filters, 3, config=cfg(), max_advances=1,
+                                                  device_match=device_match)
+    assert advances == 1 and examined == LANES * ROUNDS * SLOTS
+    texts = F.FilterSet.parse_all(filters).texts()
+    assert [(h.offset, texts[h.filter]) for h in found] == [(off1, a1), (off2, a2[:53])]
+    assert key.address(found[0].public_key) == a1

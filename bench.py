@@ -694,6 +694,15 @@ def main():
         }
         if e2e:
             line["e2e"] = e2e
+        if world > 1:
+            # the CPU baseline and the single-GPU legs (suffix, batched,
+            # serving) describe one GPU and its host: they run at N = 1 only,
+            # so that N GPUs are not held for them
+            line["legs"] = "the CPU baseline and the suffix, batched and serving legs run at N = 1 only"
+            print(json.dumps(line), flush=True)
+            if pg:
+                pg.destroy_process_group()
+            return
         line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
         if args.suite in ("default", "suffix"):
             line["suffix"] = suffix_leg(dev, 2 if args.suite == "default" else args.steps, advances)

@@ -434,6 +434,46 @@ def suffix_small_case(args):
         print(f"advance {i}: {len(o)} matches, search kernel {eng.last_kernel_ms():.3f} ms")
 
 
+def chain_pp_per_candidate(n):
+    """Partial products per candidate of the chain scheme (the config-1
+    contract, src/batch.rs:78-122): 7 multiplications for the +8G step, 4 for
+    Montgomery's trick and y / Z, and one inversion (254 squarings of 36
+    products, 11 multiplications) per n steps."""
+    return (11 * 64 * n + 11 * 64 + 254 * 36) / n
+
+
+def chain_leg(dev, peak):
+    """The chain scheme (the device restatement of BatchEngine, which config 1
+    pins bit for bit) on config 2's search at its default shape: one warm-up
+    advance, then three timed by CUDA events."""
+    from onion_gen_b200 import _native as N
+    from onion_gen_b200 import filter as F
+    from onion_gen_b200 import gpu, key, workloads
+
+    fs = F.FilterSet.parse_all([workloads.config2_prefix()])
+    words, bits = fs.index_words()
+    eng = gpu.Engine(dev, key.start_point(workloads.seed(0)), bitmap=words, bitmap_bits=bits,
+                     config=N.EngineConfig(N.SCHEME_CHAIN, 0, 0, 1, 128, 0, 0))
+    shape = eng.shape()
+    eng.advance_raw()
+    ms = 0.0
+    for _ in range(3):
+        eng.advance_raw()
+        ms += eng.last_kernel_ms()
+    rate = 3 * eng.batch() / (ms * 1e-3)
+    eng.close()
+    w = chain_pp_per_candidate(shape.half)
+    log(f"chain leg: {rate:.4e} keys/s at n = {shape.half}, {shape.lanes} lanes")
+    return {
+        "workload": "chain scheme on config 2's search (seed LE32(0), its 16-bit index), n = %d steps per lane "
+        "between inversions, %d lanes" % (shape.half, shape.lanes),
+        "keys_per_s": rate,
+        "per_candidate": w,
+        "roofline_frac": rate * w / peak,
+        "unit": "keys/s (CUDA events on the search kernel)",
+    }
+
+
 def suffix_leg(dev, steps, advances):
     """A suffix search through the filter engine (og_engine_new_filters +
     og_engine_advance_matches): the search kernel with the suffix bitmap, the
@@ -704,6 +744,8 @@ def main():
                 pg.destroy_process_group()
             return
         line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+        if args.suite == "default":
+            line["chain"] = chain_leg(dev, peak)
         if args.suite in ("default", "suffix"):
             line["suffix"] = suffix_leg(dev, 2 if args.suite == "default" else args.steps, advances)
         if args.suite in ("default", "batched", "serving"):

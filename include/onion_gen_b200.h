@@ -80,16 +80,19 @@ enum og_scheme {
 /* Launch shape of an engine. Zero fields take defaults. */
 typedef struct og_engine_config {
     uint32_t scheme;   /* og_scheme */
-    uint32_t half;     /* paired: table size, a round is 2*half+1 candidates (0: 2048).
-                          chain: n steps (0: 1024) */
+    uint32_t half;     /* paired: table size, a round is 2*half+1 candidates (0: 2048, halved
+                          down to 256 while one advance would return more than 2^26 expected
+                          survivors). chain: n steps (0: 1024) */
     uint32_t lanes;    /* lanes (independent chains), a multiple of `block`. The paired
                           kernel runs as many CTAs as are resident and they take the lanes
                           a block at a time, so its scratch is that of the resident CTAs
-                          whatever the lanes (0: eight blocks per resident CTA) */
+                          whatever the lanes (0: eight blocks per resident CTA, fewer only
+                          if half 256 still passes that survivor budget) */
     uint32_t rounds;   /* rounds per advance */
     uint32_t block;    /* threads per CUDA block, a multiple of 32 */
     uint32_t dump;     /* 1: ignore the bitmap, every candidate survives (parity runs) */
-    uint32_t room;     /* survivor records per advance; 0 sizes it from the bitmap's occupancy */
+    uint32_t room;     /* survivor records per advance; 0 sizes it from the bitmaps' occupancy:
+                          the expected count plus eight standard deviations */
 } og_engine_config;
 
 /* The same engine with an explicit shape (no tuning). `bitmap` may be NULL

@@ -223,16 +223,23 @@ int resident_lanes(int device, uint32_t scheme, uint32_t half, uint32_t block, u
     return OG_OK;
 }
 
-// Records one advance may produce: every candidate in dump mode; else four
-// times what the bitmap's measured occupancy lets through plus a floor
-// (the margin of src/gpu/mod.rs:298-312, taken from the real occupancy
-// rather than one slot per prefix, so that short prefixes cannot overflow).
+// Records one advance may produce: every candidate in dump mode; else what
+// the bitmaps' measured occupancy lets through, plus eight standard
+// deviations of its binomial spread, plus a floor. For uniform keys each
+// candidate survives with exactly that probability, so the margin is not
+// crossed in practice, and an overflow is still an error, never a
+// truncation. (src/gpu/mod.rs:298-312 sizes the room from one slot per
+// prefix, which short prefixes overflow; this takes the real occupancy.)
 size_t room_for(uint64_t batch, bool dump, double occupancy) {
     if (dump) return (size_t)batch;
     const double expected = (double)batch * occupancy;
-    const double want = 4.0 * expected + 1024.0;
+    const double want = expected + 8.0 * std::sqrt(expected) + 1024.0;
     return (size_t)std::min<double>((double)batch, std::max(4096.0, want));
 }
+
+// Expected survivors of one advance that the default shape allows: 2^26
+// records, 3.2 GB of records per advance in flight.
+constexpr double SURVIVOR_BUDGET = (double)(1u << 26);
 
 // `f` (may be null) supplies both bitmaps instead of `bitmap`: its prefix
 // index (if it has prefixes) and its suffix index (if it has suffixes).
@@ -262,10 +269,10 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
     if (cfg.block == 0) cfg.block = 128;
     if (cfg.block % 32 || cfg.block > OG_LB_THREADS)
         return fail(err, errlen, OG_E_ARG, "block %u (a multiple of 32, at most %d)", cfg.block, OG_LB_THREADS);
+    const bool auto_half = cfg.half == 0;
     if (cfg.half == 0) cfg.half = cfg.scheme == OG_SCHEME_CHAIN ? 1024 : 2048;
     if (cfg.scheme == OG_SCHEME_PAIRED && cfg.half > 2048) return fail(err, errlen, OG_E_ARG, "half %u > 2048", cfg.half);
     if (cfg.scheme == OG_SCHEME_CHAIN && cfg.half > 65536) return fail(err, errlen, OG_E_ARG, "n %u > 65536", cfg.half);
-    const uint32_t slots = cfg.scheme == OG_SCHEME_CHAIN ? cfg.half : 2 * cfg.half + 1;
     double occ = 1.0;  // the share of candidates the bitmaps let through
     if (!cfg.dump) {
         occ = 0.0;
@@ -283,16 +290,21 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
             // the persistent kernel takes lanes a block at a time: eight
             // blocks per resident CTA leave the last ones little tail
             // (measured +3.5% over two), while the scratch stays that of the
-            // resident CTAs; fewer when the survivor buffer of one advance
-            // would pass 2^24 records
+            // resident CTAs. When one advance would return more than the
+            // survivor budget, a shorter inversion batch comes first (config
+            // 3's 5 % survivors on B200: half 512 at eight waves 19.2 G keys/s,
+            // half 2048 at one wave 16.6), then fewer waves.
             uint32_t waves = 8;
-            while (waves > 1 && 4.0 * (double)resident * waves * slots * occ > (double)(1u << 24)) waves /= 2;
+            const auto expected = [&] { return (double)resident * waves * (2.0 * cfg.half + 1) * occ; };
+            while (auto_half && cfg.half > 256 && expected() > SURVIVOR_BUDGET) cfg.half /= 2;
+            while (waves > 1 && expected() > SURVIVOR_BUDGET) waves /= 2;
             cfg.lanes = resident * waves;
         } else {
             // two waves of resident blocks: the second overlaps the first's tail
             cfg.lanes = resident * 2;
         }
     }
+    const uint32_t slots = cfg.scheme == OG_SCHEME_CHAIN ? cfg.half : 2 * cfg.half + 1;
     cfg.lanes = (cfg.lanes + cfg.block - 1) / cfg.block * cfg.block;
     if (cfg.lanes > (1u << 24)) return fail(err, errlen, OG_E_ARG, "%u lanes (at most 2^24)", cfg.lanes);
     if (cfg.rounds == 0) {
@@ -300,8 +312,8 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
         cfg.rounds = (uint32_t)std::max<uint64_t>(1, (1ULL << 27) / per_round);
     }
     const double occupancy = occ;
-    // keep the survivor buffer of one advance within 2^24 records
-    while (!cfg.dump && cfg.rounds > 1 && 4.0 * (double)cfg.lanes * slots * cfg.rounds * occupancy > (double)(1u << 24))
+    // keep the expected survivors of one advance within the budget
+    while (!cfg.dump && cfg.rounds > 1 && (double)cfg.lanes * slots * cfg.rounds * occupancy > SURVIVOR_BUDGET)
         cfg.rounds /= 2;
     if ((uint64_t)cfg.rounds * slots > 0xffffffffULL) return fail(err, errlen, OG_E_ARG, "too many rounds per advance");
 

@@ -265,3 +265,26 @@ def test_reference_gpu_harness_case(device):
     assert examined == 4 * eng.batch() and len(offsets) > 0
     # a 15-bit literal on its index: about examined / 2^15 exact matches
     assert 0.5 * examined / 2**15 < confirmed < 1.5 * examined / 2**15
+
+
+def test_default_shape_for_a_dense_index(device):
+    """A set that lets 5 % of candidates through (config 3): the default keeps
+    eight waves of lanes and shortens the inversion batch until one advance's
+    expected survivors fit 2^26 records; the room holds the expected count
+    plus eight standard deviations; an advance returns about that many."""
+    resident = gpu.resident_lanes(device)
+    fs = F.FilterSet.parse_all(workloads.config3_prefixes())
+    words, bits = fs.index_words()
+    occ = fs.occupancy()
+    half = 2048
+    while half > 256 and 8 * resident * (2 * half + 1) * occ > 2**26:
+        half //= 2
+    eng = gpu.Engine(device, key.start_point(workloads.seed(0)), bitmap=words, bitmap_bits=bits,
+                     config=cfg(N.SCHEME_PAIRED, 0, 0, 1, dump=0))
+    assert eng.shape().half == half < 2048 and eng.threads() == 8 * resident
+    mu = eng.batch() * occ
+    assert mu + 7.9 * mu**0.5 < eng.room() < mu + 8.1 * mu**0.5 + 1100
+    o, k = eng.advance_raw()
+    assert abs(len(o) - mu) < 6 * mu**0.5
+    for i in range(0, len(o), len(o) // 50):
+        key.check_hit(workloads.seed(0), int(o[i]), bytes(k[i]))

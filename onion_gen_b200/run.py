@@ -89,7 +89,7 @@ UNLIMITED = 0xFFFFFFFF
 
 
 def search_lease(device, root: bytes, first_block: int, blocks: int, filters, report, keep_going=None,
-                 max_steps=None, **batch_shape):
+                 max_steps=None, rank: int = 0, world: int = 1, **batch_shape):
     """A worker's leased range (worker::search, src/worker/run.rs:167-238) on
     one GPU: blocks first_block .. first_block + blocks - 1 of `root`, each
     searched from its own seed (block_seed, src/run.rs:211-221), all of them
@@ -100,12 +100,18 @@ def search_lease(device, root: bytes, first_block: int, blocks: int, filters, re
     ends, already confirmed and re-derived on the host: positions are what
     cross the wire, as in the reference. Within a block, finds come in offset
     order. ``report`` returns whether to go on (the reference's callback does
-    the same). Returns the number of steps run."""
-    from . import batch as B
+    the same). Returns the number of steps run.
 
-    b = B.Batch(device, max_searches=max(blocks, 1), **batch_shape)
+    With one process per GPU, rank ``rank`` of ``world`` takes its share of
+    the blocks (``shard.lease_blocks``): the shares are disjoint, and nothing
+    crosses between the GPUs."""
+    from . import batch as B
+    from . import shard
+
+    mine = shard.lease_blocks(first_block, blocks, rank, world)
+    b = B.Batch(device, max_searches=max(len(mine), 1), **batch_shape)
     try:
-        for blk in range(first_block, first_block + blocks):
+        for blk in mine:
             b.admit(blk, key.block_seed(root, blk), filters, UNLIMITED)
         steps = 0
         while (keep_going is None or keep_going()) and (max_steps is None or steps < max_steps):

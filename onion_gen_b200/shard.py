@@ -28,6 +28,17 @@ def global_offset(rank: int, offset: int) -> int:
     return (rank << RANK_SHIFT) + offset
 
 
+def lease_blocks(first_block: int, blocks: int, rank: int, world: int):
+    """The blocks of a leased range one rank searches: every world-th block,
+    starting at first_block + rank. Each block is searched from its own seed
+    (block_seed), as the reference's device workers each take blocks of the
+    lease (src/run.rs:1040-1049); the ranks' shares are disjoint and cover
+    the range."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError(f"rank {rank} of {world}")
+    return list(range(first_block + rank, first_block + blocks, world))
+
+
 def max_over_ranks(values, group=None):
     """Element-wise maximum of per-rank timings (torch.distributed, any backend)."""
     import torch

@@ -229,3 +229,22 @@ def test_a_leased_range_reports_every_block_s_finds_in_order(device):
             assert fs.match_address(pk) is not None
         found, _, _ = run.device_search(device, seed, filters, len(offs), config=cfg)
         assert [h.offset for h in found] == offs
+
+
+def test_a_lease_split_over_ranks_finds_the_same_hits(device):
+    """search_lease as rank 1 of 2 takes block 401 of the range 400..402 only;
+    its finds are the same first hits of that block's seed that the whole
+    range searched by one rank reports (both are prefixes of one sequence)."""
+    root = bytes(range(32))
+    filters = ["ab", "q7"]
+    whole, part = {}, {}
+
+    def into(d):
+        return lambda block, offset: d.setdefault(block, []).append(offset) or True
+
+    run.search_lease(device, root, 400, 3, filters, into(whole), max_steps=6, half=64, slots=128 * 64)
+    run.search_lease(device, root, 400, 3, filters, into(part), max_steps=6, rank=1, world=2, half=64,
+                     slots=128 * 64)
+    assert sorted(part) == [401]
+    n = min(len(part[401]), len(whole[401]))
+    assert n > 0 and part[401][:n] == whole[401][:n]

@@ -80,10 +80,11 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--case", default="full", choices=["full", "small", "batch-small", "suffix-small"],
+    p.add_argument("--case", default="full", choices=["full", "small", "batch-small", "suffix-small", "chain-small"],
                    help="small: the profiling case, three one-round advances of the plain engine; "
                    "batch-small: three steps of the batched engine over the first 16 config-4 searches; "
-                   "suffix-small: three advances of a forty-suffix search with the device match")
+                   "suffix-small: three advances of a forty-suffix search with the device match; "
+                   "chain-small: three advances of the chain scheme at its default shape")
     p.add_argument("--half", type=int, default=0,
                    help=f"inversion batch half-width (default {HALF} for the plain line, 256 for --case small, "
                    f"{SHORT_HALF} for the batch's profiling case)")
@@ -416,6 +417,26 @@ def small_case(args):
               f"{eng.batch() / ms * 1e3:.4e} keys/s")
 
 
+def chain_small_case(args):
+    """Three advances of the chain scheme on config 2's search at its default
+    shape (n = 1024, two waves of lanes): the case the chain kernel's ncu
+    summary is captured on."""
+    from onion_gen_b200 import _native as N
+    from onion_gen_b200 import filter as F
+    from onion_gen_b200 import gpu, key, workloads
+
+    dev = gpu.look()[0]
+    fs = F.FilterSet.parse_all([workloads.config2_prefix()])
+    words, bits = fs.index_words()
+    eng = gpu.Engine(dev, key.start_point(workloads.seed(0)), bitmap=words, bitmap_bits=bits,
+                     config=N.EngineConfig(N.SCHEME_CHAIN, args.half, 0, 1, 128, 0, 0))
+    for i in range(3):
+        o, _ = eng.advance_raw()
+        ms = eng.last_kernel_ms()
+        print(f"advance {i}: n {eng.shape().half}, {eng.threads()} lanes, {len(o)} survivors, kernel {ms:.3f} ms, "
+              f"{eng.batch() / ms * 1e3:.4e} keys/s")
+
+
 def suffix_small_case(args):
     """Three advances of a suffix search (og_engine_new_filters, forty
     eight-symbol suffixes, half 256, one resident wave): the case the suffix
@@ -553,6 +574,9 @@ def main():
         return
     if args.case == "suffix-small":
         suffix_small_case(args)
+        return
+    if args.case == "chain-small":
+        chain_small_case(args)
         return
     rank, world, local = dist_env()
     import ctypes as C

@@ -288,3 +288,19 @@ def test_default_shape_for_a_dense_index(device):
     assert abs(len(o) - mu) < 6 * mu**0.5
     for i in range(0, len(o), len(o) // 50):
         key.check_hit(workloads.seed(0), int(o[i]), bytes(k[i]))
+
+
+@pytest.mark.parametrize("block", [32, 96])
+def test_paired_smaller_blocks_tile_the_range(oracle, device, block):
+    """Blocks of 32 and 96 threads (the ABI takes any multiple of 32 up to
+    128): the persistent CTAs, the parked centres and the scratch slots are
+    per block, and two advances still tile the range bit-exactly."""
+    start = oracle_start(oracle, workloads.seed(13))
+    lanes = 4 * 96
+    eng = gpu.Engine(device, start, config=cfg(N.SCHEME_PAIRED, 48, lanes, 2, block=block))
+    assert eng.shape().block == block and eng.threads() == lanes
+    offs, keys = sorted_run(eng, advances=2)
+    n = 2 * lanes * (2 * 48 + 1) * 2
+    assert np.array_equal(offs, 8 * (1 + np.arange(n, dtype=np.uint64)))
+    want = np.frombuffer(oracle.chain_keys_mt(start, 1, n), dtype=np.uint8).reshape(-1, 32)
+    assert np.array_equal(keys, want)

@@ -203,3 +203,24 @@ def test_full_address_filters(device, device_match):
     texts = F.FilterSet.parse_all(filters).texts()
     assert [(h.offset, texts[h.filter]) for h in found] == [(off1, a1), (off2, a2[:53])]
     assert key.address(found[0].public_key) == a1
+
+
+def test_chain_scheme_device_match_equals_host_match(device):
+    """The chain scheme (scheme 1) with the device match: the same matches,
+    offsets and filter indices as the host's match of its survivors, on
+    literal prefixes of config 3 plus patterns."""
+    start = key.start_point(workloads.seed(4))
+    fs = F.FilterSet.parse_all(workloads.config3_prefixes(1500) + ["a?c", "[xyz]2k"])
+    words, bits = fs.index_words()
+    chain = N.EngineConfig(N.SCHEME_CHAIN, 256, 1024, 2, 128, 0, 0)
+    plain = gpu.Engine(device, start, bitmap=words, bitmap_bits=bits, config=chain)
+    want = host_matches(plain, fs, 2)
+    plain.close()
+    matched = gpu.Engine(device, start, bitmap=words, bitmap_bits=bits, config=chain)
+    matched.match_on_device(fs)
+    got = device_matches(matched, 2)
+    matched.close()
+    assert len(want) > 100 and got == want
+    for o, packed, f in got[:50]:
+        pk, _ = key.check_hit(workloads.seed(4), o, packed)
+        assert fs.match_address(pk) == f

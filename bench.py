@@ -419,7 +419,7 @@ def small_case(args):
 
 def chain_small_case(args):
     """Three advances of the chain scheme on config 2's search at its default
-    shape (n = 1024, two waves of lanes): the case the chain kernel's ncu
+    shape (n = 1024, four waves of lanes): the case the chain kernel's ncu
     summary is captured on."""
     from onion_gen_b200 import _native as N
     from onion_gen_b200 import filter as F
@@ -465,8 +465,9 @@ def chain_pp_per_candidate(n):
 
 def chain_leg(dev, peak):
     """The chain scheme (the device restatement of BatchEngine, which config 1
-    pins bit for bit) on config 2's search at its default shape: one warm-up
-    advance, then three timed by CUDA events."""
+    pins bit for bit) on config 2's search at its default shape (n = 1024,
+    four waves of lanes): one warm-up advance, then three timed by CUDA
+    events."""
     from onion_gen_b200 import _native as N
     from onion_gen_b200 import filter as F
     from onion_gen_b200 import gpu, key, workloads

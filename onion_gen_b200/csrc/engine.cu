@@ -300,8 +300,12 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
             while (waves > 1 && expected() > SURVIVOR_BUDGET) waves /= 2;
             cfg.lanes = resident * waves;
         } else {
-            // two waves of resident blocks: the second overlaps the first's tail
-            cfg.lanes = resident * 2;
+            // persistent too: four waves of resident blocks (on B200 at
+            // n = 1024: 9.05 G keys/s for the earlier one-lane-per-thread
+            // kernel at two waves; persistent, over two runs, 9.19-9.25 /
+            // 9.31-9.37 / 9.20-9.54 at 2 / 4 / 8 waves, all on the scratch
+            // of one wave)
+            cfg.lanes = resident * 4;
         }
     }
     const uint32_t slots = cfg.scheme == OG_SCHEME_CHAIN ? cfg.half : 2 * cfg.half + 1;
@@ -341,15 +345,15 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
     const uint32_t coords = cfg.scheme == OG_SCHEME_CHAIN ? 4 : 2;
     CU(e->lanes.alloc(L * coords * 2));
     const size_t elems = cfg.scheme == OG_SCHEME_CHAIN ? cfg.half : 2 * (size_t)cfg.half + 2;
-    if (cfg.scheme == OG_SCHEME_PAIRED) {
-        // the paired kernel is persistent: scratch for the resident CTAs only
+    {
+        // both kernels are persistent: scratch for the resident CTAs only
+        // (the chain kernel's no more CTAs than blocks of lanes)
         uint32_t resident = 0;
         int rc = resident_lanes(ordinal, cfg.scheme, cfg.half, cfg.block, &resident, err, errlen);
         if (rc) return rc;
         e->grid = std::max<uint32_t>(1, resident / cfg.block);
+        if (cfg.scheme == OG_SCHEME_CHAIN) e->grid = std::min<uint32_t>(e->grid, (uint32_t)(L / cfg.block));
         CU(e->scratch.alloc((size_t)e->grid * cfg.block * elems * 4));
-    } else {
-        CU(e->scratch.alloc(L * elems * 4));
     }
     for (og_engine::Flight& f : e->fl) {
         CU(f.counts.alloc(4));
@@ -429,6 +433,8 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
         ChainArgs& a = e->ca;
         a.lanes = e->lanes.p;
         a.scratch = e->scratch.p;
+        a.work = nullptr;  // the flight's counter, set per launch
+        a.slots_n = e->grid * cfg.block;
         a.bitmap = cfg.dump ? nullptr : e->bitmap.p;
         a.bits = bits;
         a.sbitmap = e->sbitmap.p;
@@ -565,7 +571,8 @@ int enqueue_advance(og_engine* e, bool match, char* err, size_t errlen) {
     } else {
         e->ca.hits = f.hits.p;
         e->ca.counter = f.counts.p;
-        CU(launch_chain(e->ca, (int)e->cfg.block, e->stream));
+        e->ca.work = f.counts.p + 3;
+        CU(launch_chain(e->ca, (int)e->cfg.block, (int)e->grid, e->stream));
     }
     CU(cudaEventRecord(f.ev1, e->stream));
     if (match) {

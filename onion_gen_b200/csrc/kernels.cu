@@ -76,42 +76,53 @@ __global__ void __launch_bounds__(OG_LB_THREADS, OG_LB_MIN_BLOCKS) paired_kernel
     }
 }
 
-// the chain kernel (parity contract, not the production path) keeps 96 registers: at 80 it spills
+// The chain kernel (the config-1 contract) keeps 96 registers: at 80 it
+// spills. Persistent like the paired kernel: each CTA takes the next block
+// of lanes until none is left, and the scratch is indexed by the CTA's
+// slot, so any number of waves of lanes costs the scratch of one.
 __global__ void __launch_bounds__(OG_LB_THREADS, 5) chain_kernel(const ChainArgs a) {
-    const uint32_t lane = blockIdx.x * blockDim.x + threadIdx.x;
-    const size_t L = a.lanes_n;
+    __shared__ uint32_t item_s;
+    const size_t L = a.lanes_n, S = a.slots_n;
+    const uint32_t nblocks = a.lanes_n / blockDim.x;
     const Sink sink{a.bitmap, a.bits, a.hits, a.counter, a.cap, a.search, a.sbitmap, a.sbits};
-    uint4* const scr = a.scratch + lane;
-#define SCR(e, w) (scr + ((size_t)(e) * 4 + (w) * 2) * L)
-    fe X = load_fe(a.lanes + 0 * L + lane, L);
-    fe Y = load_fe(a.lanes + 2 * L + lane, L);
-    fe Z = load_fe(a.lanes + 4 * L + lane, L);
-    fe T = load_fe(a.lanes + 6 * L + lane, L);
-    const fe sp = words_fe(a.step_ypx), sm = words_fe(a.step_ymx), st = words_fe(a.step_t2d);
-    for (uint32_t r = 0; r < a.rounds; r++) {
-        fe run = fe_one();
+    uint4* const scr = a.scratch + (blockIdx.x * blockDim.x + threadIdx.x);
+#define SCR(e, w) (scr + ((size_t)(e) * 4 + (w) * 2) * S)
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) item_s = atomicAdd(a.work, 1u);
+        __syncthreads();
+        const uint32_t item = item_s;
+        if (item >= nblocks) break;
+        const uint32_t lane = item * blockDim.x + threadIdx.x;
+        fe X = load_fe(a.lanes + 0 * L + lane, L);
+        fe Y = load_fe(a.lanes + 2 * L + lane, L);
+        fe Z = load_fe(a.lanes + 4 * L + lane, L);
+        fe T = load_fe(a.lanes + 6 * L + lane, L);
+        for (uint32_t r = 0; r < a.rounds; r++) {
+            fe run = fe_one();
 #pragma unroll 1
-        for (uint32_t t = 0; t < a.n; t++) {
-            store_fe(SCR(t, 0), L, fe_mulv(Y, run));
-            store_fe(SCR(t, 1), L, Z);
-            run = fe_mulv(run, Z);
-            add_cached(X, Y, Z, T, sp, sm, st);
-        }
-        if (L > 1) add_cached(X, Y, Z, T, words_fe(a.jump_ypx), words_fe(a.jump_ymx), words_fe(a.jump_t2d));
-        fe acc = fe_invert(run);
-        const uint32_t base_step = r * a.n;
+            for (uint32_t t = 0; t < a.n; t++) {
+                store_fe(SCR(t, 0), S, fe_mulv(Y, run));
+                store_fe(SCR(t, 1), S, Z);
+                run = fe_mulv(run, Z);
+                add_cached(X, Y, Z, T, words_fe(a.step_ypx), words_fe(a.step_ymx), words_fe(a.step_t2d));
+            }
+            if (L > 1) add_cached(X, Y, Z, T, words_fe(a.jump_ypx), words_fe(a.jump_ymx), words_fe(a.jump_t2d));
+            fe acc = fe_invert(run);
+            const uint32_t base_step = r * a.n;
 #pragma unroll 1
-        for (uint32_t t = a.n; t-- > 0;) {
-            const fe v = fe_mulv(load_fe(SCR(t, 0), L), acc);
-            acc = fe_mulv(acc, load_fe(SCR(t, 1), L));
-            test_emit(sink, v, lane, base_step + t);
+            for (uint32_t t = a.n; t-- > 0;) {
+                const fe v = fe_mulv(load_fe(SCR(t, 0), S), acc);
+                acc = fe_mulv(acc, load_fe(SCR(t, 1), S));
+                test_emit(sink, v, lane, base_step + t);
+            }
         }
+        store_fe(a.lanes + 0 * L + lane, L, X);
+        store_fe(a.lanes + 2 * L + lane, L, Y);
+        store_fe(a.lanes + 4 * L + lane, L, Z);
+        store_fe(a.lanes + 6 * L + lane, L, T);
     }
 #undef SCR
-    store_fe(a.lanes + 0 * L + lane, L, X);
-    store_fe(a.lanes + 2 * L + lane, L, Y);
-    store_fe(a.lanes + 4 * L + lane, L, Z);
-    store_fe(a.lanes + 6 * L + lane, L, T);
 }
 
 // The filter a suffix-bitmap survivor matches (suffix_match), with the
@@ -169,9 +180,10 @@ cudaError_t launch_paired(const PairedArgs& a, int block, int grid, cudaStream_t
     return cudaGetLastError();
 }
 
-cudaError_t launch_chain(const ChainArgs& a, int block, cudaStream_t s) {
-    if (a.lanes_n % block != 0 || block % 32 != 0) return cudaErrorInvalidValue;
-    chain_kernel<<<a.lanes_n / block, block, 0, s>>>(a);
+cudaError_t launch_chain(const ChainArgs& a, int block, int grid, cudaStream_t s) {
+    if (a.lanes_n % block != 0 || block % 32 != 0 || grid < 1 || (uint32_t)grid * block != a.slots_n)
+        return cudaErrorInvalidValue;
+    chain_kernel<<<grid, block, 0, s>>>(a);
     return cudaGetLastError();
 }
 

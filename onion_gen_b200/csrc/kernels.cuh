@@ -66,7 +66,9 @@ struct PairedArgs {
 
 struct ChainArgs {
     uint4* lanes;            // projective points: ({X,Y,Z,T} * 2 + q) * L + lane
-    uint4* scratch;          // ((t * 2 + {num,den}) * 2 + q) * L + lane, t < n
+    uint4* scratch;          // ((t * 2 + {num,den}) * 2 + q) * S + slot, t < n (per persistent CTA slot)
+    uint32_t* work;          // blocks of lanes taken so far this launch (starts at 0)
+    uint32_t slots_n;        // S = persistent CTAs x block
     const uint32_t* bitmap;
     uint32_t bits;
     HitRec* hits;
@@ -151,7 +153,7 @@ cudaError_t launch_match(const MatchArgs& a, int grid, cudaStream_t s);
 // lanes a block at a time from `work`, so the scratch covers only the lanes
 // in flight and no SM idles in a tail wave.
 cudaError_t launch_paired(const PairedArgs& a, int block, int grid, cudaStream_t s);
-cudaError_t launch_chain(const ChainArgs& a, int block, cudaStream_t s);
+cudaError_t launch_chain(const ChainArgs& a, int block, int grid, cudaStream_t s);
 
 // Register and shared-memory footprint of the search kernels, for the shape
 // choice.

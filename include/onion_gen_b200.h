@@ -87,7 +87,8 @@ typedef struct og_engine_config {
                           kernel runs as many CTAs as are resident and they take the lanes
                           a block at a time, so its scratch is that of the resident CTAs
                           whatever the lanes (0: eight blocks per resident CTA, fewer only
-                          if half 256 still passes that survivor budget) */
+                          if half 256 still passes that survivor budget). The chain kernel is
+                          persistent the same way (0: four blocks per resident CTA) */
     uint32_t rounds;   /* rounds per advance */
     uint32_t block;    /* threads per CUDA block, a multiple of 32 */
     uint32_t dump;     /* 1: ignore the bitmap, every candidate survives (parity runs) */

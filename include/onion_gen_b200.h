@@ -355,10 +355,12 @@ void og_serve_free(og_serve* s);
  * w = (step / (2 half + 1)) * lanes + lane and i = step % (2 half + 1).
  *
  * Limits: lanes a multiple of 128, half <= 2048, and
- * lanes * (2 half + 3) * 64 + (half + 24) * 96 <= OG_NOALLOC_SCRATCH_BYTES;
+ * lanes * (2 half + 3) * 64 + half * 96 <= OG_NOALLOC_SCRATCH_BYTES;
  * beyond that the call fails with OG_E_CAPACITY before touching the device.
  * Work is enqueued on `stream` (a cudaStream_t; NULL for the legacy default
- * stream) and the call returns without waiting for it.
+ * stream) and the call returns without waiting for it: it enqueues one
+ * memset of `*d_count` and three kernels, whose constants travel as launch
+ * parameters, and copies nothing from host memory.
  *
  * The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress); make that first call before any stream capture.

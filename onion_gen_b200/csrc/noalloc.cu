@@ -36,15 +36,22 @@ constexpr int MAX_DEVICES = 64;
 static __device__ __align__(256) uint4 og_noalloc_scratch[SCRATCH_BYTES / sizeof(uint4)];
 
 // Layout inside the array, in uint4 units: the table Q_m (half * 6), the
-// lane-start powers of two (POW2 * 6), the lane centres (lanes * 4) and the
-// Montgomery scratch (lanes * (2 half + 2) * 4).
+// lane centres (lanes * 4) and the Montgomery scratch
+// (lanes * (2 half + 2) * 4).
 size_t need_uint4(uint32_t lanes, uint32_t half) {
-    return (size_t)half * 6 + (size_t)POW2 * 6 + (size_t)lanes * 4 + (size_t)lanes * (2 * (size_t)half + 2) * 4;
+    return (size_t)half * 6 + (size_t)lanes * 4 + (size_t)lanes * (2 * (size_t)half + 2) * 4;
 }
+
+// 2^k p for k < POW2 in cached form (y + x, y - x, 2 d x y; Z = 1), passed to
+// the kernels by value as a launch parameter (2304 bytes), so that the call
+// copies nothing from host memory: a host-to-device copy from pageable
+// memory would wait for the work already queued on the caller's stream.
+struct Pow2Table {
+    uint4 v[POW2 * 6];
+};
 
 struct NoAllocArgs {
     uint4* table;
-    uint4* pow2;
     uint4* lanes;
     uint4* scratch;
     FeWords bx, by, bz, bt;  // first centre, extended
@@ -63,13 +70,13 @@ struct NoAllocArgs {
 // The table Q_m = m * 8G, m = 1..half, affine with x y. Entry m - 1 starts
 // from 8G and adds 2^k * 8G (from `pow8`) for every bit k of m - 1, then is
 // normalised.
-__global__ void __launch_bounds__(NBLOCK) noalloc_table_kernel(const NoAllocArgs a, const uint4* pow8) {
+__global__ void __launch_bounds__(NBLOCK) noalloc_table_kernel(const NoAllocArgs a, const Pow2Table pow8) {
     const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= a.half) return;
     fe X = words_fe(a.ex), Y = words_fe(a.ey), Z = words_fe(a.ez), T = words_fe(a.et);
     for (uint32_t k = 0; k < POW2; k++)
         if ((m >> k) & 1u) {
-            const uint4* p = pow8 + (size_t)k * 6;
+            const uint4* p = pow8.v + (size_t)k * 6;
             add_cached(X, Y, Z, T, load_fe(p + 0, 1), load_fe(p + 2, 1), load_fe(p + 4, 1));
         }
     const fe zi = fe_invert(Z);
@@ -80,14 +87,16 @@ __global__ void __launch_bounds__(NBLOCK) noalloc_table_kernel(const NoAllocArgs
     store_fe(d + 4, 1, fe_mulv(x, y));
 }
 
-__global__ void __launch_bounds__(NBLOCK) noalloc_init_kernel(const NoAllocArgs a) {
+// Lane l starts on the centre of window l: the first centre plus 2^k times
+// the lane stride (from `pow2`) for every bit k of l.
+__global__ void __launch_bounds__(NBLOCK) noalloc_init_kernel(const NoAllocArgs a, const Pow2Table pow2) {
     const uint32_t lane = blockIdx.x * blockDim.x + threadIdx.x;
     if (lane >= a.lanes_n) return;
     const size_t L = a.lanes_n;
     fe X = words_fe(a.bx), Y = words_fe(a.by), Z = words_fe(a.bz), T = words_fe(a.bt);
     for (uint32_t k = 0; k < POW2; k++)
         if ((lane >> k) & 1u) {
-            const uint4* p = a.pow2 + (size_t)k * 6;
+            const uint4* p = pow2.v + (size_t)k * 6;
             add_cached(X, Y, Z, T, load_fe(p + 0, 1), load_fe(p + 2, 1), load_fe(p + 4, 1));
         }
     const fe zi = fe_invert(Z);
@@ -112,8 +121,8 @@ __global__ void __launch_bounds__(NBLOCK, 5) noalloc_paired_kernel(const NoAlloc
 std::mutex g_mu;
 uint4* g_addr[MAX_DEVICES];
 
-// 2^k * p for k < POW2 in cached form, into a caller-provided host array.
-void pow2_into(Pt p, uint4 out[POW2 * 6]) {
+// 2^k * p for k < POW2 in cached form.
+void pow2_into(Pt p, uint4* out) {
     for (uint32_t k = 0; k < POW2; k++) {
         const Niels c = pt_niels(p);
         put_fe(out + k * 6 + 0, 1, c.ypx);
@@ -144,7 +153,7 @@ extern "C" int og_search_noalloc(int ordinal, const uint8_t start[128], uint32_t
     if (need > SCRATCH_BYTES)
         return fail(err, errlen, OG_E_CAPACITY,
                     "%u lanes at half %u need %zu bytes of scratch; the fixed array holds %zu "
-                    "(lanes * (2 half + 3) * 64 + (half + 24) * 96 must stay within it)",
+                    "(lanes * (2 half + 3) * 64 + half * 96 must stay within it)",
                     lanes, half, need, SCRATCH_BYTES);
     const Pt A = point_from_bytes(start);
     if (!point_valid(A)) return fail(err, errlen, OG_E_ARG, "the start point is not on the curve");
@@ -166,11 +175,11 @@ extern "C" int og_search_noalloc(int ordinal, const uint8_t start[128], uint32_t
     NoAllocArgs a;
     std::memset(&a, 0, sizeof a);
     a.table = base;
-    a.pow2 = a.table + (size_t)half * 6;
-    a.lanes = a.pow2 + (size_t)POW2 * 6;
+    a.lanes = a.table + (size_t)half * 6;
     a.scratch = a.lanes + (size_t)lanes * 4;
     const uint32_t slots = 2 * half + 1;
-    // host constants, on the stack: the first centre, 8G, the round stride
+    // constants computed on the host and passed as launch parameters: the
+    // first centre, 8G, the round stride
     const Pt first = pt_add(A, base_mult_u64(8ULL * (half + 1)));
     a.bx = to_words(first.X);
     a.by = to_words(first.Y);
@@ -194,22 +203,15 @@ extern "C" int og_search_noalloc(int ordinal, const uint8_t start[128], uint32_t
     a.lanes_n = lanes;
     a.half = half;
     a.rounds = rounds;
-    // two power-of-two tables go into the array: the lane stride's in its
-    // own region, and 8G's (used only to build the table) in the scratch
-    // region, which nothing reads or writes before the paired kernel
-    uint4 host_pow[POW2 * 6];
-    pow2_into(base_mult_u64(8ULL * slots), host_pow);
-    e = cudaMemcpyAsync(a.pow2, host_pow, sizeof host_pow, cudaMemcpyHostToDevice, s);
-    if (e != cudaSuccess) return fail(err, errlen, OG_E_DEVICE, "copy: %s", cuda_text(e).c_str());
-    uint4* pow8 = a.scratch;
-    pow2_into(eight, host_pow);
-    e = cudaMemcpyAsync(pow8, host_pow, sizeof host_pow, cudaMemcpyHostToDevice, s);
-    if (e != cudaSuccess) return fail(err, errlen, OG_E_DEVICE, "copy: %s", cuda_text(e).c_str());
+    // the two power-of-two tables travel as launch parameters
+    Pow2Table pow2, pow8;
+    pow2_into(base_mult_u64(8ULL * slots), pow2.v);
+    pow2_into(eight, pow8.v);
     // the counter starts at zero on every call
     e = cudaMemsetAsync(d_count, 0, sizeof(uint32_t), s);
     if (e != cudaSuccess) return fail(err, errlen, OG_E_DEVICE, "memset: %s", cuda_text(e).c_str());
     noalloc_table_kernel<<<(half + NBLOCK - 1) / NBLOCK, NBLOCK, 0, s>>>(a, pow8);
-    noalloc_init_kernel<<<lanes / NBLOCK, NBLOCK, 0, s>>>(a);
+    noalloc_init_kernel<<<lanes / NBLOCK, NBLOCK, 0, s>>>(a, pow2);
     noalloc_paired_kernel<<<lanes / NBLOCK, NBLOCK, 0, s>>>(a);
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail(err, errlen, OG_E_DEVICE, "launch: %s", cuda_text(e).c_str());

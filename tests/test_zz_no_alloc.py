@@ -9,9 +9,13 @@ buffers they already own; the library's scratch is a fixed device array.
 Checked on a B200 (-m gpu) through the C ABI against og_engine_advance on a
 fresh engine of the same shape: the same survivors, bit for bit, on two calls
 in a row (a filtered one, then one that keeps every candidate), then the
-first again. This file is collected last, so a run that stops at the first
+first again; and a call made behind a finite spin kernel on the same stream
+returns before that kernel ends (it copies nothing from host memory, so it
+does not wait for queued work). This file is collected last, so a run that stops at the first
 failure has run every other test before it.
 """
+import time
+
 import numpy as np
 import pytest
 import torch
@@ -34,13 +38,13 @@ def with_engine(device, start, words, bits, dump):
     return sorted(zip(offsets.tolist(), (bytes(p) for p in packed)))
 
 
-def without_allocation(device, start, d_bitmap, bits, cap):
+def without_allocation(device, start, d_bitmap, bits, cap, stream=None):
     # the caller's own device buffers: survivor records and their counter
     d_hits = torch.zeros(cap * 12, dtype=torch.int32, device=f"cuda:{device.ordinal}")
     d_count = torch.full((1,), 12345, dtype=torch.int32, device=f"cuda:{device.ordinal}")
     err = N.errbuf()
     rc = N.lib.og_search_noalloc(
-        device.ordinal, start, LANES, HALF, ROUNDS, d_bitmap, bits, d_hits.data_ptr(), cap, d_count.data_ptr(), None,
+        device.ordinal, start, LANES, HALF, ROUNDS, d_bitmap, bits, d_hits.data_ptr(), cap, d_count.data_ptr(), stream,
         err, 512,
     )
     N.check(rc, err)
@@ -86,3 +90,34 @@ def test_no_allocation_entry_point_refuses_sizes_beyond_its_array(device):
                                  d_count.data_ptr(), None, err, 512)
     assert N.STATUS[rc] == "OG_E_CAPACITY"
     assert b"fixed array" in err.value
+
+
+def test_no_allocation_entry_point_returns_without_waiting_for_queued_work(device):
+    fs = F.FilterSet.parse_all(["ab", "q7"])
+    words, bits = fs.index_words()
+    dev = f"cuda:{device.ordinal}"
+    d_bitmap = torch.from_numpy(words.view(np.int64)).to(dev)
+    start = key.start_point(workloads.seed(3))
+    n = LANES * ROUNDS * SLOTS
+    want = without_allocation(device, start, d_bitmap.data_ptr(), bits, cap=n)  # the device's first call done
+    stream = torch.cuda.Stream(device=dev)
+    d_hits = torch.zeros(n * 12, dtype=torch.int32, device=dev)
+    d_count = torch.zeros(1, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        torch.cuda._sleep(1_000_000_000)  # a finite spin of about half a second at B200 clocks
+    err = N.errbuf()
+    t0 = time.perf_counter()
+    rc = N.lib.og_search_noalloc(device.ordinal, start, LANES, HALF, ROUNDS, d_bitmap.data_ptr(), bits,
+                                 d_hits.data_ptr(), n, d_count.data_ptr(), stream.cuda_stream, err, 512)
+    returned_s = time.perf_counter() - t0
+    still_queued = not stream.query()
+    N.check(rc, err)
+    stream.synchronize()
+    assert still_queued, "the spin kernel had ended before the call returned"
+    assert returned_s < 0.1
+    m = int(d_count.item())
+    recs = d_hits[: m * 12].cpu().numpy().view(np.uint32).reshape(m, 12)
+    got = sorted((8 * (((int(r[1]) // SLOTS) * LANES + int(r[0])) * SLOTS + 1 + int(r[1]) % SLOTS),
+                  r[4:12].astype("<u4").tobytes()) for r in recs)
+    assert got == want

@@ -27,14 +27,21 @@ One JSON line on rank 0:
   batch_shape the batch's autotuner (og_batch_tune): inversion batch,
               slot pool and grid, the fastest within 8 ms a step; the
               batched and serving legs run that shape
-  batched     config 4 (64 searches, 1..5000 prefixes of 4..7 symbols, quota
-              1..16): the single-search engine one search at a time (the
-              run driver's loop) against the batched engine, same results;
-              the default run takes the searches whose expected work is at
-              most --batched-cap candidates, --suite batched all of them
-  serving     config 5 (Poisson arrivals at 50/s, 1..200 prefixes, quota
-              1..16) through the serving loop: p50/p99 time-to-find over the
-              requests completed within a wall-clock cap
+  config3     config 3 (10,000 prefixes of 3..8 symbols, a 24-bit index, 2^32
+              candidates a step) with the exact match on the device: kernel
+              keys/s and its roofline fraction, and end to end with every
+              match copied back and a sample re-derived on the host
+  batched     config 4 (all 64 searches, 1..5000 prefixes of 4..7 symbols,
+              quota 1..16): the single-search engine one search at a time
+              (the run driver's loop), once with the reference-shaped
+              constructor's tuned shape and once at half 256, against the
+              batched engine (long searches at a larger inversion batch, two
+              steps in flight); same results
+  serving     config 5 (all 2000 requests, Poisson arrivals at 50/s, 1..200
+              prefixes, quota 1..16) through the serving loop under a
+              wall-clock cap: p50/p99 time-to-find over all requests, a
+              request unfinished at the cap counted at its elapsed time as a
+              lower bound (censored)
 
 --impl reference times that CPU engine alone (the reference's GPU engine is
 Rust compiled to PTX by a nightly toolchain that is not available here).
@@ -45,12 +52,15 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
 import sys
 import threading
 import time
+
+import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
@@ -85,16 +95,19 @@ def parse():
                    "batch-small: three steps of the batched engine over the first 16 config-4 searches; "
                    "suffix-small: three advances of a forty-suffix search with the device match; "
                    "chain-small: three advances of the chain scheme at its default shape")
+    p.add_argument("--lanes-per-thread", type=int, default=1,
+                   help="lanes each thread of the paired search kernel carries in --case small (1 or 2)")
     p.add_argument("--half", type=int, default=0,
                    help=f"inversion batch half-width (default {HALF} for the plain line, 256 for --case small, "
                    f"{SHORT_HALF} for the batch's profiling case)")
-    p.add_argument("--suite", default="default", choices=["default", "batched", "serving", "plain", "suffix"],
-                   help="default: the plain line plus bounded suffix, batched and serving legs; "
-                   "batched / serving / suffix: that leg at full size; plain: the plain line only")
-    p.add_argument("--batched-cap", type=float, default=2e10,
-                   help="largest expected work (candidates) of a config-4 search in the default run")
-    p.add_argument("--serving-requests", type=int, default=400)
-    p.add_argument("--serving-cap", type=float, default=20.0, help="serving wall-clock cap, seconds")
+    p.add_argument("--suite", default="default",
+                   choices=["default", "batched", "serving", "plain", "suffix", "config3"],
+                   help="default: the plain line plus the chain, suffix, config-3, batched and serving legs; "
+                   "batched / serving / suffix / config3: that leg alone; plain: the plain line only")
+    p.add_argument("--batched-cap", type=float, default=float("inf"),
+                   help="largest expected work (candidates) of a config-4 search to run (default: all)")
+    p.add_argument("--serving-requests", type=int, default=2000)
+    p.add_argument("--serving-cap", type=float, default=60.0, help="serving wall-clock cap, seconds")
     return p.parse_args()
 
 
@@ -281,32 +294,66 @@ def batch_shape(dev):
                    "tune_s": time.perf_counter() - t0}
 
 
+# config-4 searches whose expected work is above this many candidates are
+# the "long" ones (two of the 64: 2.4e11 and 4.1e11 expected candidates)
+LONG_SEARCH = 2e10
+
+
+def plain_arm(dev, searches, config):
+    """The run driver's loop (src/run.rs:1036-1074): one engine per search,
+    one search at a time, until its quota of verified hits."""
+    from onion_gen_b200 import run
+
+    out, examined, launches, per = {}, 0, 0, {}
+    t0 = time.perf_counter()
+    for s in searches:
+        t1 = time.perf_counter()
+        found, ex, advances = run.device_search(dev, s.seed, s.prefixes, s.quota, config=config)
+        per[s.index] = time.perf_counter() - t1
+        out[s.index] = [(h.offset, h.packed) for h in found]
+        examined += ex
+        launches += 2 * advances + 1
+    wall = time.perf_counter() - t0
+    long_s = sum(t for i, t in per.items() if searches_by_index(searches)[i].expected_candidates() > LONG_SEARCH)
+    return out, {"wall_s": wall, "examined": examined, "examined_per_s": examined / wall, "gpu_launches": launches,
+                 "long_searches_wall_s": long_s, "short_searches_wall_s": wall - long_s}
+
+
+def searches_by_index(searches):
+    return {s.index: s for s in searches}
+
+
 def batched_leg(dev, shape, cap):
-    """Config 4: plain (one engine per search) against batched, same searches."""
+    """Config 4: the plain engine (one engine per search, the run driver's
+    loop) against the batched engine, same searches, same results."""
     from onion_gen_b200 import _native as N
     from onion_gen_b200 import batch as B
-    from onion_gen_b200 import gpu, run, workloads
+    from onion_gen_b200 import gpu, key, workloads
 
     all_searches = workloads.config4_searches()
     searches = [s for s in all_searches if s.expected_candidates() <= cap]
-    # one search at a time, as the run driver does: half 256 and one lane per
-    # thread of two waves of resident blocks (1.2e8 candidates an advance), so
-    # that a small search does not overshoot its quota by much
-    cfg = N.EngineConfig(N.SCHEME_PAIRED, SHORT_HALF, 2 * gpu.resident_lanes(dev), 0, 128, 0, 0)
-    t0 = time.perf_counter()
-    plain, plain_examined, plain_launches = {}, 0, 0
-    for s in searches:
-        found, examined, advances = run.device_search(dev, s.seed, s.prefixes, s.quota, config=cfg)
-        plain[s.index] = [(h.offset, h.packed) for h in found]
-        plain_examined += examined
-        plain_launches += 2 * advances + 1
-    plain_wall = time.perf_counter() - t0
-    log(f"batched leg: plain engine {len(searches)} searches in {plain_wall:.2f} s")
+    # the reference-shaped constructor (og_engine_new, threads = 0) takes its
+    # shape from tuning.yaml, timing the candidates once if there is none:
+    # that walk runs here, before the clock
+    probe = gpu.Engine(dev, key.start_point(workloads.seed(0)), threads=0,
+                       bitmap=np.zeros(1024, dtype=np.uint64), bitmap_bits=16)
+    tuned = probe.shape()
+    probe.close()
+    tuned_shape = {"half": tuned.half, "lanes": tuned.lanes, "rounds": tuned.rounds,
+                   "candidates_per_advance": tuned.lanes * (2 * tuned.half + 1) * tuned.rounds}
+    plain_tuned, arm_tuned = plain_arm(dev, searches, None)
+    log(f"batched leg: plain engine (tuned shape {tuned_shape}) {len(searches)} searches in {arm_tuned['wall_s']:.2f} s")
+    # the same loop with a short round (half 256, two waves of resident
+    # blocks: 9.7e7 candidates an advance), which overshoots a small quota less
+    short = N.EngineConfig(N.SCHEME_PAIRED, SHORT_HALF, 2 * gpu.resident_lanes(dev), 1, 128, 0, 0)
+    plain_short, arm_short = plain_arm(dev, searches, short)
+    log(f"batched leg: plain engine (half {SHORT_HALF}) in {arm_short['wall_s']:.2f} s")
 
     t0 = time.perf_counter()
-    b = B.Batch(dev, **shape)
+    b = B.Batch(dev, **shape, max_half=HALF)
     for s in searches:
         b.admit(s.index, s.seed, s.prefixes, s.quota)
+    halves = {s.index: b.status(s.index).half for s in searches}
     steps = launches = 0
     dev_ms = 0.0
     examined = 0
@@ -321,68 +368,172 @@ def batched_leg(dev, shape, cap):
     batched_wall = time.perf_counter() - t0
     log(f"batched leg: batched engine in {batched_wall:.2f} s, {steps} steps")
     useful = sum(r[-1][0] // 8 for r in batched.values())
+    long_ids = [s.index for s in searches if s.expected_candidates() > LONG_SEARCH]
+    useful_long = sum(batched[i][-1][0] // 8 for i in long_ids)
+    for arm in (arm_tuned, arm_short):
+        arm["keys_per_s"] = useful / arm["wall_s"]
+    best_plain = min(arm_tuned["wall_s"], arm_short["wall_s"])
+    best_name = "tuned" if arm_tuned["wall_s"] <= arm_short["wall_s"] else f"half {SHORT_HALF}"
+    best_arm = arm_tuned if best_name == "tuned" else arm_short
     return {
         "workload": "config 4: 64 searches, seeds LE32(j), 1..5000 prefixes (log-uniform) of 4..7 symbols, "
-        "quota 1..16; searches with expected work <= %.0e candidates" % cap,
+        "quota 1..16" + ("" if cap == float("inf") else "; searches with expected work <= %.0e candidates" % cap),
         "searches": len(searches),
         "searches_in_config": len(all_searches),
         "expected_candidates": sum(s.expected_candidates() for s in searches),
         "candidates_to_quota": useful,
-        "results_identical": plain == batched,
-        "plain": {"wall_s": plain_wall, "examined": plain_examined, "keys_per_s": useful / plain_wall,
-                  "examined_per_s": plain_examined / plain_wall, "gpu_launches": plain_launches},
+        "results_identical": plain_tuned == batched and plain_short == batched,
+        "plain_tuned": {"shape": tuned_shape, "constructor": "og_engine_new(threads = 0), the tuned shape", **arm_tuned},
+        "plain_half256": {"shape": {"half": SHORT_HALF, "lanes": short.lanes, "rounds": 1},
+                          "constructor": "og_engine_new_config", **arm_short},
         "batched": {"wall_s": batched_wall, "examined": examined, "keys_per_s": useful / batched_wall,
                     "examined_per_s": examined / batched_wall, "device_s": dev_ms / 1e3, "steps": steps,
-                    "gpu_launches": launches},
-        "speedup_batched_over_plain": plain_wall / batched_wall,
+                    "gpu_launches": launches, "halves": sorted(set(halves.values())),
+                    "long_search_halves": [halves[i] for i in long_ids],
+                    "shape": {**shape, "max_half": HALF, "inflight": 2}},
+        "speedup_batched_over_plain": best_plain / batched_wall,
+        "speedup_against": f"the faster plain arm ({best_name})",
+        "speedup_over_plain_tuned": arm_tuned["wall_s"] / batched_wall,
+        "speedup_over_plain_half256": arm_short["wall_s"] / batched_wall,
+        "long_searches": {
+            "count": len(long_ids),
+            "candidates_to_quota": useful_long,
+            "share_of_work": useful_long / useful,
+            "plain_wall_s": best_arm["long_searches_wall_s"],
+            "bound_note": "a batch runs a long search no faster than the plain engine's own rate, so even with "
+            "the short searches free the speedup over that plain arm is at most wall / long_searches wall",
+            "speedup_bound": best_plain / best_arm["long_searches_wall_s"] if best_arm["long_searches_wall_s"] else None,
+        },
         "unit": "keys/s (candidates up to each search's quota-th hit, wall clock)",
     }
 
 
 def serving_leg(dev, shape, n, cap_s):
-    """Config 5: requests submitted at their Poisson arrival times."""
+    """Config 5: requests submitted at their Poisson arrival times, served
+    until all complete or the wall-clock cap. Time-to-find is completion
+    minus arrival; a request still queued or running at the cap has taken at
+    least the cap's end minus its arrival, and enters the percentiles with
+    that lower bound (a censored value)."""
     from onion_gen_b200 import serve, workloads
 
     reqs = workloads.config5_requests(n)
     s = serve.Server(dev, **shape)
     t0 = s.now_ns()
     submitted = 0
+    sub_ns = {}
     done = {}
     while True:
         now = (s.now_ns() - t0) / 1e9
         while submitted < n and reqs[submitted].arrival <= now:
             r = reqs[submitted]
             s.submit(r.index, r.seed, r.prefixes, r.quota)
+            sub_ns[r.index] = s.now_ns()
             submitted += 1
         for d in s.poll():
             done[d.request_id] = d
         if len(done) == n or now > cap_s:
             break
         time.sleep(0.002)
-    elapsed = (s.now_ns() - t0) / 1e9
+    end_ns = s.now_ns()
+    elapsed = (end_ns - t0) / 1e9
     log(f"serving leg: {len(done)} of {submitted} done in {elapsed:.1f} s")
     st = s.stats()
     s.close()
     ok = [d for d in done.values() if d.status == 0]
-    ttf = sorted((d.done_ns - d.arrival_ns) / 1e9 for d in ok)
+    failed = [d for d in done.values() if d.status != 0]
+    # (seconds, censored): completed exactly; unfinished at least end - arrival
+    ttf = [((d.done_ns - d.arrival_ns) / 1e9, False) for d in ok]
+    ttf += [((end_ns - sub_ns[r.index]) / 1e9, True) for r in reqs[:submitted] if r.index not in done]
+    ttf.sort()
 
     def q(p):
-        return ttf[min(len(ttf) - 1, int(p * len(ttf)))] if ttf else None
+        if not ttf:
+            return None, None
+        v, c = ttf[min(len(ttf) - 1, max(0, math.ceil(p * len(ttf)) - 1))]
+        return v, c
 
+    p50, c50 = q(0.50)
+    p99, c99 = q(0.99)
     return {
-        "workload": f"config 5: first {n} of 2000 requests, Poisson arrivals at 50/s (splitmix64(5)), "
+        "workload": f"config 5: {n} requests, Poisson arrivals at 50/s (splitmix64(5)), "
         "1..200 prefixes (log-uniform) of 4..7 symbols, quota 1..16",
         "submitted": submitted,
         "completed": len(ok),
+        "failed": len(failed),
+        "unfinished_at_cap": submitted - len(done),
         "wall_cap_s": cap_s,
         "elapsed_s": elapsed,
-        "p50_ttf_s": q(0.50),
-        "p99_ttf_s": q(0.99),
-        "ttf_note": "over the requests completed within the cap; the mix's total expected work exceeds what "
-        "one GPU examines in the cap, so the longest requests are still running when it ends",
+        "p50_ttf_s": p50,
+        "p50_censored": c50,
+        "p99_ttf_s": p99,
+        "p99_censored": c99,
+        "ttf_note": "percentiles over all submitted requests; a request unfinished at the cap counts with its "
+        "elapsed time (cap end - arrival), a lower bound, and a percentile that lands on one is marked censored. "
+        "The mix's expected work (2.4e13 candidates, 20 minutes of one GPU) is about 30 times what arrives per "
+        "second of capacity, so its longest requests cannot finish within the cap",
         "keys_per_s": st.candidates / elapsed,
         "device_busy": st.device_ms / 1e3 / elapsed,
         "steps": int(st.steps),
+    }
+
+
+def config3_leg(dev, peak, steps=2):
+    """Config 3 on its default shape with the exact match on the device: the
+    search kernel's keys/s (CUDA events) and roofline fraction, and the same
+    candidates end to end through the engine's launch/collect with every
+    match copied back and a sample of them re-derived on the host."""
+    from onion_gen_b200 import _native as N
+    from onion_gen_b200 import filter as F
+    from onion_gen_b200 import gpu, key, workloads
+
+    prefixes = workloads.config3_prefixes()
+    fs = F.FilterSet.parse_all(prefixes)
+    words, bits = fs.index_words()
+    seed = workloads.seed(0)
+    eng = gpu.Engine(dev, key.start_point(seed), bitmap=words, bitmap_bits=bits,
+                     config=N.EngineConfig(N.SCHEME_PAIRED, 0, 0, 0, 128, 0, 0))
+    eng.match_on_device(fs)
+    shape = eng.shape()
+    batch = eng.batch()
+    advances = -(-CANDIDATES_PER_STEP // batch)
+    eng.advance_matches_raw()  # warm-up
+    kernel_ms = 0.0
+    matches = checked = 0
+    rng = np.random.default_rng(3)
+    t0 = time.perf_counter()
+    total = steps * advances
+    launched = 0
+    for i in range(total):
+        while launched - i < 2 and launched < total:
+            eng.launch_matches()
+            launched += 1
+        o, k, f = eng.collect_matches_raw()
+        kernel_ms += eng.last_kernel_ms()
+        matches += len(o)
+        for j in rng.choice(len(o), size=min(64, len(o)), replace=False):
+            pk, _ = key.check_hit(seed, int(o[j]), bytes(k[j]))
+            if fs.match_address(pk) != int(f[j]):
+                raise RuntimeError(f"config 3: match at offset {int(o[j])} does not confirm on the host")
+            checked += 1
+    wall = time.perf_counter() - t0
+    eng.close()
+    n = batch * total
+    w = pp_per_candidate(shape.half)
+    rate = n / (kernel_ms * 1e-3)
+    log(f"config 3 leg: {rate:.4e} keys/s device, {n / wall:.4e} end to end, {matches} matches")
+    return {
+        "workload": "config 3: seed LE32(0), 10,000 prefixes of 3..8 symbols (splitmix64(3)), "
+        f"{bits}-bit index, {steps} steps of 2^32 candidates (rounded up to whole advances), device exact match",
+        "shape": {"half": shape.half, "lanes": shape.lanes, "rounds": shape.rounds, "advances_per_step": advances},
+        "candidates": n,
+        "keys_per_s": rate,
+        "roofline_frac": rate * w / peak,
+        "per_candidate": w,
+        "e2e_keys_per_s": n / wall,
+        "matches": matches,
+        "match_fraction": matches / n,
+        "matches_rederived": checked,
+        "unit": "keys/s (CUDA events on the search kernel; e2e: wall clock with every match copied back)",
     }
 
 
@@ -405,15 +556,18 @@ def small_case(args):
 
     dev = gpu.look()[0]
     half = args.half or 256
-    lanes = gpu.resident_lanes(dev) * 8
+    lpt = args.lanes_per_thread
     fs = F.FilterSet.parse_all([workloads.config2_prefix()])
     words, bits = fs.index_words()
     start = key.start_point(workloads.seed(0))
-    eng = gpu.Engine(dev, start, bitmap=words, bitmap_bits=bits, config=N.EngineConfig(0, half, lanes, 1, 128, 0, 0))
+    # eight blocks of lanes per resident CTA (lanes 0: the engine's default waves)
+    eng = gpu.Engine(dev, start, bitmap=words, bitmap_bits=bits,
+                     config=N.EngineConfig(0, half, 0, 1, 128, 0, 0, lpt))
+    lanes = eng.threads()
     for i in range(3):
         o, _ = eng.advance_raw()
         ms = eng.last_kernel_ms()
-        print(f"advance {i}: half {half}, {lanes} lanes, {len(o)} survivors, kernel {ms:.3f} ms, "
+        print(f"advance {i}: half {half}, {lanes} lanes ({lpt} a thread), {len(o)} survivors, kernel {ms:.3f} ms, "
               f"{eng.batch() / ms * 1e3:.4e} keys/s")
 
 
@@ -582,7 +736,6 @@ def main():
     rank, world, local = dist_env()
     import ctypes as C
 
-    import numpy as np
     import torch
 
     from onion_gen_b200 import _native as N
@@ -660,6 +813,8 @@ def main():
         hbm_peak = 6650.0  # the pool's earlier measurement, when the driver's file is absent
     achieved = value / world * w
     peak = imad.value / 2.0
+    clock_summary = clocks.summary()
+    theoretical = (dev.sms * 32 * clock_summary["sm_mhz"] * 1e6) if clock_summary.get("sm_mhz") else None
 
     # end to end through the C ABI, host buffers, every hit re-derived. As
     # the reference's device worker (src/run.rs:1030-1119) does, one engine
@@ -753,6 +908,10 @@ def main():
                 "traffic_unit": "DRAM bytes per launch (ncu, dram__bytes_read.sum + dram__bytes_write.sum)",
                 "per_candidate": w,
                 "peak_source": "measured: og_measure_int_peak mad.lo.u32 issue rate / 2 (lo+hi per product)",
+                "peak_theoretical": theoretical,
+                "peak_theoretical_source": "SMs x 32 wide 32x32->64 multiply-adds a clock (fmaheavy) x the median "
+                "SM clock sampled during the timed steps",
+                "frac_of_theoretical": achieved / theoretical if theoretical else None,
                 "fe_mul_pp_per_s": mulpp.value,
                 "hbm": {
                     "achieved": value / world * ALGORITHMIC_BYTES_PER_CANDIDATE / 1e9,
@@ -762,7 +921,7 @@ def main():
                     "note": "the Montgomery scratch: not the bound",
                 },
             },
-            "clocks": clocks.summary(),
+            "clocks": clock_summary,
         }
         if e2e:
             line["e2e"] = e2e
@@ -780,15 +939,14 @@ def main():
             line["chain"] = chain_leg(dev, peak)
         if args.suite in ("default", "suffix"):
             line["suffix"] = suffix_leg(dev, 2 if args.suite == "default" else args.steps, advances)
+        if args.suite in ("default", "config3"):
+            line["config3"] = config3_leg(dev, peak)
         if args.suite in ("default", "batched", "serving"):
             shape, line["batch_shape"] = batch_shape(dev)
         if args.suite in ("default", "batched"):
-            cap = args.batched_cap if args.suite == "default" else float("inf")
-            line["batched"] = batched_leg(dev, shape, cap)
+            line["batched"] = batched_leg(dev, shape, args.batched_cap)
         if args.suite in ("default", "serving"):
-            n = args.serving_requests if args.suite == "default" else 2000
-            cap = args.serving_cap if args.suite == "default" else 120.0
-            line["serving"] = serving_leg(dev, shape, n, cap)
+            line["serving"] = serving_leg(dev, shape, args.serving_requests, args.serving_cap)
         print(json.dumps(line), flush=True)
     if pg:
         pg.destroy_process_group()

@@ -94,6 +94,8 @@ typedef struct og_engine_config {
     uint32_t dump;     /* 1: ignore the bitmap, every candidate survives (parity runs) */
     uint32_t room;     /* survivor records per advance; 0 sizes it from the bitmaps' occupancy:
                           the expected count plus eight standard deviations */
+    uint32_t lanes_per_thread; /* paired: lanes each thread of the search kernel carries, 1 or 2
+                          (0: 1); `lanes` is then a multiple of block x this. Chain: 1 */
 } og_engine_config;
 
 /* The same engine with an explicit shape (no tuning). `bitmap` may be NULL
@@ -212,6 +214,13 @@ typedef struct og_batch_config {
     uint32_t graph;         /* 0 or 1: replay each step as a captured CUDA graph; 2: plain launches */
     uint32_t grid;          /* persistent CTAs per SM (0: as many as fit) */
     uint64_t memory_budget; /* device bytes for per-search tables (0: half of the free memory after the pool) */
+    uint32_t max_half;      /* largest inversion batch a search may run at (0: `half`): a search runs at
+                               half doubled while its expected work (quota over its filters' match
+                               probability) covers at least four steps of the whole pool at the doubled
+                               half; a power-of-two multiple of `half`, at most 2048 */
+    uint32_t inflight;      /* steps queued on the device at once, 1 or 2 (0: 2): og_batch_step
+                               launches the next step before it collects the oldest, so the host's
+                               work on one step's hits overlaps the next step */
 } og_batch_config;
 
 typedef struct og_batch_hit {
@@ -232,6 +241,9 @@ typedef struct og_search_status {
     uint32_t done;       /* 1 once the first `quota` hits are known */
     uint32_t filters;
     uint64_t table_bytes;/* device bytes of its bitmap and exact-match tables */
+    uint32_t status;     /* OG_OK, or OG_E_VERIFY when one of its device hits did not re-derive on
+                            the host (it is then done, with the hits verified before) */
+    uint32_t half;       /* its inversion batch */
 } og_search_status;
 
 int og_batch_new(int ordinal, const og_batch_config* cfg, og_batch** out, char* err, size_t errlen);
@@ -258,13 +270,26 @@ void og_batch_shape(const og_batch* b, og_batch_config* cfg);
 int og_batch_admit(og_batch* b, uint64_t search_id, const uint8_t seed[32], const char* filters, uint32_t quota,
                    char* err, size_t errlen);
 /* One step: every admitted, unfinished search advances `rounds` rounds.
- * Writes this step's verified hits to `out` (room `cap`, og_batch_room()). */
+ * With `inflight` 2 the call first launches the next step (so that up to two
+ * are queued on the device), then waits for the oldest and writes its
+ * verified hits to `out` (room `cap`; `out` NULL: none are copied, they stay
+ * in og_batch_results); a search whose quota
+ * the oldest step meets may still hold lanes in the newer one, and the device
+ * skips them. Errors:
+ *   OG_E_VERIFY   a device hit of some searches did not re-derive on the host:
+ *                 those searches end (og_search_status.status), the other
+ *                 searches' hits of the step are in `out`, and the batch goes on;
+ *   OG_E_OVERFLOW a step's survivors or hits exceeded their room: the batch
+ *                 closes, and every later call fails with OG_E_STATE;
+ *   OG_E_DEVICE   a CUDA call failed: the batch closes likewise. */
 int og_batch_step(og_batch* b, og_batch_hit* out, size_t cap, size_t* n, char* err, size_t errlen);
 size_t og_batch_room(const og_batch* b);
 int og_batch_status(const og_batch* b, uint64_t search_id, og_search_status* st);
 /* The result of a finished search: its first `quota` hits in offset order. */
 int og_batch_results(const og_batch* b, uint64_t search_id, og_batch_hit* out, size_t cap, size_t* n);
-/* Removes a search (finished or not) and frees its lanes and tables. */
+/* Removes a search (finished or not) and frees its lanes and tables. The
+ * tables go back to the batch's pool in stream order, after the steps
+ * already launched: the call does not wait for the device. */
 int og_batch_retire(og_batch* b, uint64_t search_id);
 /* Searches admitted and not yet retired; of them, unfinished. */
 void og_batch_counts(const og_batch* b, size_t* admitted, size_t* running);
@@ -276,6 +301,10 @@ uint64_t og_batch_last_step_candidates(const og_batch* b);
 uint32_t og_batch_last_step_launches(const og_batch* b);
 /* Device bytes of per-search tables in use, and the budget. */
 void og_batch_memory(const og_batch* b, uint64_t* used, uint64_t* budget);
+/* For tests of the failure path: the host treats the next hit of the search
+ * that it verifies as one that did not re-derive. The fault is made on the
+ * host; nothing on the device changes. */
+int og_batch_plant_mismatch(og_batch* b, uint64_t search_id);
 void og_batch_free(og_batch* b);
 
 /* ---- serving: a request loop over the batched engine -------------------

@@ -55,6 +55,7 @@ class EngineConfig(C.Structure):
         ("block", C.c_uint32),
         ("dump", C.c_uint32),
         ("room", C.c_uint32),
+        ("lanes_per_thread", C.c_uint32),
     ]
 
 
@@ -68,6 +69,8 @@ class BatchConfig(C.Structure):
         ("graph", C.c_uint32),
         ("grid", C.c_uint32),
         ("memory_budget", C.c_uint64),
+        ("max_half", C.c_uint32),
+        ("inflight", C.c_uint32),
     ]
 
 
@@ -92,6 +95,8 @@ class SearchStatus(C.Structure):
         ("done", C.c_uint32),
         ("filters", C.c_uint32),
         ("table_bytes", C.c_uint64),
+        ("status", C.c_uint32),
+        ("half", C.c_uint32),
     ]
 
 
@@ -173,6 +178,7 @@ def _load():
     sig("og_batch_last_step_candidates", U64, [P])
     sig("og_batch_last_step_launches", U32, [P])
     sig("og_batch_memory", None, [P, C.POINTER(U64), C.POINTER(U64)])
+    sig("og_batch_plant_mismatch", I, [P, U64])
     sig("og_batch_free", None, [P])
     sig("og_serve_new", I, [I, C.POINTER(ServeConfig), C.POINTER(P), B, SZ])
     sig("og_serve_submit", I, [P, U64, B, B, U32, B, SZ])

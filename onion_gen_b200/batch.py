@@ -8,8 +8,11 @@
 
 Each step replays one captured CUDA graph: lane initialisation, one
 persistent search kernel over every search's lanes, and the device-side
-exact match; every hit is re-derived on the host before it counts. A
-search's result does not depend on what else runs beside it.
+exact match; every hit is re-derived on the host before it counts. Two
+steps are in flight by default: ``step()`` launches the next one before it
+collects the oldest. A search's result does not depend on what else runs
+beside it, nor on its inversion batch (``max_half`` lets long searches run
+at a larger one).
 """
 from __future__ import annotations
 
@@ -28,20 +31,27 @@ class Hit:
     filter: int
 
 
+STEP_ROOM = 1 << 20
+
+
 def _hit(h: N.BatchHit) -> Hit:
     return Hit(h.search_id, h.offset, bytes(h.packed), bytes(h.public_key), h.filter)
 
 
 class Batch:
     def __init__(self, device=0, half=0, slots=0, rounds=0, max_searches=0, max_hits=0, graph=True, memory_budget=0,
-                 grid=0):
+                 grid=0, max_half=0, inflight=0):
         ordinal = getattr(device, "ordinal", device)
-        cfg = N.BatchConfig(half, slots, rounds, max_searches, max_hits, 1 if graph else 2, grid, memory_budget)
+        cfg = N.BatchConfig(half, slots, rounds, max_searches, max_hits, 1 if graph else 2, grid, memory_budget,
+                            max_half, inflight)
         h = C.c_void_p()
         err = N.errbuf()
         N.check(N.lib.og_batch_new(int(ordinal), C.byref(cfg), C.byref(h), err, 512), err)
         self._h = h
-        self._room = N.lib.og_batch_room(h)
+        # verified hits one step returns: at most the quotas of the running
+        # searches, far below the device's room for exact hits; a step with
+        # more fails with OG_E_CAPACITY (the batch keeps them in results())
+        self._room = min(N.lib.og_batch_room(h), STEP_ROOM)
         self._buf = (N.BatchHit * self._room)()
 
     def close(self):
@@ -111,6 +121,13 @@ class Batch:
 
     def last_step_launches(self) -> int:
         return N.lib.og_batch_last_step_launches(self._h)
+
+    def plant_mismatch(self, search_id: int) -> None:
+        """Tests only: the next hit of the search the host verifies counts as
+        one that did not re-derive (the search then ends with OG_E_VERIFY)."""
+        rc = N.lib.og_batch_plant_mismatch(self._h, search_id)
+        if rc:
+            raise N.OgError(rc, f"search {search_id}")
 
     def memory(self):
         u, b = C.c_uint64(), C.c_uint64()

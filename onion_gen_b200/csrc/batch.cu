@@ -2,30 +2,45 @@
 // kernel, replayed as a CUDA graph per step. No counterpart in the reference;
 // the per-search arithmetic is the single engine's paired round.
 //
-// Candidate windows. Window w of a search is the round centred on
-// scalar offset 8 (w (2 half + 1) + half + 1): its 2 half + 1 candidates are
-// offsets 8 (w (2 half + 1) + 1 + i), i in [0, 2 half]. A search holding L
-// lanes for a step of R rounds processes windows [W, W + R L) — lane l takes
-// W + r L + l in round r — and ends the step with lane l centred on window
-// W + R L + l. So after every step lane l sits on window W_done + l whatever
-// L was: a search that grows only initialises its new lanes, one that
-// shrinks drops its highest lanes, and the windows it has processed are
-// always exactly [0, W_done).
+// Candidate windows. A search runs at its own inversion batch `half`; its
+// window w is the round centred on scalar offset 8 (w (2 half + 1) + half + 1),
+// whose 2 half + 1 candidates are offsets 8 (w (2 half + 1) + 1 + i),
+// i in [0, 2 half]. A search holding L lanes for a step of R rounds processes
+// windows [W, W + R L) — lane l takes W + r L + l in round r — and ends the
+// step with lane l centred on window W + R L + l. So after every step lane l
+// sits on window W_done + l whatever L was: a search that grows only
+// initialises its new lanes, one that shrinks drops its highest lanes, and
+// the windows it has processed are always exactly [0, W_done).
 //
 // Results. A search is done when it holds `quota` verified hits; because its
 // windows are processed in increasing order, these are its first `quota`
-// hits in offset order, a pure function of the search alone.
+// hits in offset order, a pure function of the search alone (whatever its
+// half, lanes or neighbours).
+//
+// Steps in flight. og_batch_step keeps up to `inflight` steps queued on the
+// device (two by default): it launches the next step, then collects the
+// oldest one (waits for it, copies its exact hits back on a stream of their
+// own and re-derives them on the host) while the newer one runs. A step is
+// planned from what the host knows when it launches it, so a search that
+// meets its quota in the step still in flight keeps its lanes for one more
+// step. The device does not run them: the exact-match kernel counts every
+// search's exact hits, and the search kernel returns at once from a block of
+// a search whose count has reached its quota. Per-search tables come from a
+// stream-ordered pool and are freed in stream order, so admitting or
+// retiring a search never waits for the device.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <array>
+#include <cmath>
 #include <cstddef>
 #include <cstring>
 #include <map>
 #include <memory>
-#include <mutex>
 #include <new>
+#include <set>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/onion_gen_b200.h"
@@ -57,25 +72,33 @@ constexpr uint32_t BLOCK = 128;
 constexpr uint32_t NONE = 0xffffffffu;
 constexpr int MAX_BUCKETS = MAX_MATCH_BUCKETS;
 constexpr uint32_t POW2_BITS = 24;  // lanes of one search stay below 2^24
+constexpr uint32_t MAX_HALF = 2048;
+constexpr int FLIGHTS = 2;
 // A filter set whose bitmap lets more than this fraction of candidates
 // through is refused: the survivor buffer is sized from it.
 constexpr double MAX_OCCUPANCY = 0.02;
+// With max_half above half, a search runs at a doubled half while its
+// expected work covers at least this many steps of the whole pool there.
+constexpr double LONG_STEPS = 4.0;
 
 struct BatchDesc {
     FeWords wx, wy, wt;      // the search's stride for this step: L (2 half + 1) 8 G, affine
     FeWords bx, by, bz, bt;  // centre of window W_done (where new lanes start), extended
     const uint32_t* bitmap;  // prefix bitmap (nullptr: the search has no prefix)
     uint32_t bits;
+    uint32_t half;           // the search's inversion batch: a round is 2 half + 1 candidates
     MatchTables match;
     const uint32_t* sbitmap;  // suffix bitmap (nullptr: no suffix)
     uint32_t sbits;
     uint32_t prefix_count;    // filter index of suffix j is prefix_count + j
     const uint32_t* suffixes; // the suffix patterns (SuffixTables layout)
     uint32_t nsuffix;
+    uint32_t quota;           // exact hits after which the device skips the search's blocks (0: never)
+    const uint4* pow2;        // 2^k (2 half + 1) 8 G, k < POW2_BITS, cached: new lanes' start points
     FeWords sx, sy, sz, st;   // the search's start point s B, extended
 };
 
-// Where a search stands in this step: the windows done before it and the
+// Where a search stands in a step: the windows done before it and the
 // lanes it runs (a survivor's offset is decoded from them on the device).
 struct SearchPos {
     uint64_t windows;
@@ -101,21 +124,21 @@ struct BatchArgs {
     const BatchDesc* descs;
     const SlotBlock* blocks;
     const uint32_t* init_list;
-    Counters* counters;
+    Counters* counters;  // the flight's
     uint32_t nblocks;
-    uint4* lanes;  // ({x,y} * 2 + q) * slots + slot
+    uint4* lanes;    // ({x,y} * 2 + q) * slots + slot
     uint4* scratch;  // per persistent CTA thread: ((e * 2 + w) * 2 + q) * grid * BLOCK + cta slot
     size_t slots;
-    const uint4* table;
-    const uint4* pow2;
-    uint32_t half;
+    const uint4* table;  // Q_m, m = 1..max half; a search of half h reads the first h
     uint32_t rounds;
-    HitRec* surv;
+    HitRec* surv;  // the flight's
     uint32_t surv_cap;
-    HitRec* hits;
+    HitRec* hits;  // the flight's
     uint32_t hit_cap;
     const SearchPos* pos;  // per descriptor
     const uint4* pow8;     // 2^j 8G, j < 64, for the suffix key recomputation
+    uint32_t* found;       // per descriptor: exact hits counted on the device so far
+    uint32_t* mism;        // per descriptor: suffix survivors whose recomputed key differed
 };
 
 __global__ void __launch_bounds__(BLOCK) batch_init_kernel(const BatchArgs a) {
@@ -128,7 +151,7 @@ __global__ void __launch_bounds__(BLOCK) batch_init_kernel(const BatchArgs a) {
     fe X = words_fe(d.bx), Y = words_fe(d.by), Z = words_fe(d.bz), T = words_fe(d.bt);
     for (uint32_t k = 0; k < POW2_BITS; k++) {
         if ((lane >> k) & 1u) {
-            const uint4* p = a.pow2 + (size_t)k * 6;
+            const uint4* p = d.pow2 + (size_t)k * 6;
             add_cached(X, Y, Z, T, load_fe(p + 0, 1), load_fe(p + 2, 1), load_fe(p + 4, 1));
         }
     }
@@ -139,7 +162,9 @@ __global__ void __launch_bounds__(BLOCK) batch_init_kernel(const BatchArgs a) {
 
 // Persistent: one CTA per resident slot, each pulling slot blocks until the
 // pool is exhausted. Every block of lanes belongs to one search, whose
-// descriptor gives its stride and bitmap.
+// descriptor gives its half, stride and bitmap. A block of a search whose
+// exact hits have reached its quota (counted by the previous steps' exact
+// kernels) is skipped: its lanes stay where they are.
 __global__ void __launch_bounds__(OG_LB_THREADS, OG_LB_MIN_BLOCKS) batch_search_kernel(const BatchArgs a) {
     const uint4* qtab = a.table;  // read through L1, as the single-search kernel does
     __shared__ uint32_t item_s;
@@ -152,11 +177,12 @@ __global__ void __launch_bounds__(OG_LB_THREADS, OG_LB_MIN_BLOCKS) batch_search_
         const SlotBlock sb = a.blocks[item];
         if (sb.sidx == NONE) continue;
         const BatchDesc& d = a.descs[sb.sidx];
+        if (d.quota && a.found[sb.sidx] >= d.quota) continue;
         const uint32_t slot = item * BLOCK + threadIdx.x;
         const Sink sink{d.bitmap, d.bits, a.surv, &a.counters->surv, a.surv_cap, sb.sidx, d.sbitmap, d.sbits};
         fe x = load_fe(a.lanes + 0 * a.slots + slot, a.slots);
         fe y = load_fe(a.lanes + 2 * a.slots + slot, a.slots);
-        paired_rounds<false>(x, y, words_fe(d.wx), words_fe(d.wy), words_fe(d.wt), qtab, a.half, a.rounds,
+        paired_rounds<false>(x, y, words_fe(d.wx), words_fe(d.wy), words_fe(d.wt), qtab, d.half, a.rounds,
                       a.scratch + (blockIdx.x * BLOCK + threadIdx.x), (size_t)gridDim.x * BLOCK,
                       [&](const fe& v, uint32_t step) { test_emit(sink, v, slot, step); });
         store_fe(a.lanes + 0 * a.slots + slot, a.slots, x);
@@ -165,7 +191,8 @@ __global__ void __launch_bounds__(OG_LB_THREADS, OG_LB_MIN_BLOCKS) batch_search_
 }
 
 // Exact match of the bitmap survivors: per distinct filter length, a binary
-// search of the sorted masked key heads (FilterSet::match_key on the device).
+// search of the sorted masked key heads (FilterSet::match_key on the device);
+// every exact hit is counted for its search.
 __global__ void __launch_bounds__(256) batch_exact_kernel(const BatchArgs a) {
     const uint32_t n = min(a.counters->surv, a.surv_cap);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -182,16 +209,22 @@ __global__ void __launch_bounds__(256) batch_exact_kernel(const BatchArgs a) {
                 // W_done + r L + l; its candidate i has scalar offset
                 // 8 (w (2 half + 1) + 1 + i)
                 const SearchPos p = a.pos[r.search];
-                const uint32_t slots = 2 * a.half + 1;
+                const uint32_t slots = 2 * d.half + 1;
                 const uint64_t lane = a.blocks[r.lane / BLOCK].lane0 + r.lane % BLOCK;
                 const uint64_t w = p.windows + (uint64_t)(r.step / slots) * p.lanes + lane;
                 const uint64_t k = w * slots + 1 + r.step % slots;
                 const SuffixTables t{d.suffixes, d.nsuffix, a.pow8};
-                const uint32_t j = suffix_match(t, d.sx, d.sy, d.sz, d.st, k, r.y, &a.counters->mismatch);
+                bool bad = false;
+                const uint32_t j = suffix_match(t, d.sx, d.sy, d.sz, d.st, k, r.y, bad);
+                if (bad) {
+                    atomicAdd(&a.counters->mismatch, 1u);
+                    atomicAdd(a.mism + r.search, 1u);
+                }
                 if (j != NONE) owner = d.prefix_count + j;
             }
         }
         if (owner != NONE) {
+            atomicAdd(a.found + r.search, 1u);
             const uint32_t idx = atomicAdd(&a.counters->hits, 1u);
             if (idx < a.hit_cap) {
                 HitRec h = r;
@@ -210,6 +243,36 @@ std::string batch_key(int ordinal) {
     return device_key(name, "cuda-batch", 0);
 }
 
+// A device allocation from the batch's stream-ordered pool: allocated on the
+// upload stream, freed in the order of the engine's stream, so that a step
+// still in flight keeps reading it until it ends.
+template <typename T>
+struct PoolBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaStream_t free_on = nullptr;
+    PoolBuf() = default;
+    PoolBuf(const PoolBuf&) = delete;
+    PoolBuf& operator=(const PoolBuf&) = delete;
+    ~PoolBuf() { reset(); }
+    cudaError_t alloc(size_t count, cudaMemPool_t pool, cudaStream_t on, cudaStream_t free_stream) {
+        reset();
+        if (count == 0) return cudaSuccess;
+        void* q = nullptr;
+        cudaError_t e = cudaMallocFromPoolAsync(&q, count * sizeof(T), pool, on);
+        if (e != cudaSuccess) return e;
+        p = static_cast<T*>(q);
+        n = count;
+        free_on = free_stream;
+        return cudaSuccess;
+    }
+    void reset() {
+        if (p) cudaFreeAsync(p, free_on);
+        p = nullptr;
+        n = 0;
+    }
+};
+
 struct Search {
     uint64_t id = 0;
     uint8_t seed[32];
@@ -219,22 +282,60 @@ struct Search {
     SuffixSet sfx;
     bool has_prefixes = false;
     bool has_suffixes = false;
-    bool long_filters = false;
+    bool long_filters = false;  // some hit needs the host's confirmation beyond the device match
     uint32_t quota = 0;
+    uint32_t half = 0;
     uint32_t sidx = NONE;
-    DevBuf<uint32_t> bitmap;
-    DevBuf<uint64_t> keys;
-    DevBuf<uint32_t> owners;
-    DevBuf<uint32_t> sbitmap, suffixes, patterns;
+    PoolBuf<uint32_t> bitmap;
+    PoolBuf<uint64_t> keys;
+    PoolBuf<uint32_t> owners;
+    PoolBuf<uint32_t> sbitmap, suffixes, patterns;
     std::vector<FilterSet::DeviceBucket> buckets;
     uint64_t table_bytes = 0;
-    uint64_t windows = 0;           // W_done
-    std::vector<uint32_t> blocks;   // slot blocks held, in lane order
-    uint32_t lanes_last = 0;        // lanes held in the last step
-    uint32_t lanes_stride = 0;      // lane count the descriptor's stride is for
-    std::vector<og_batch_hit> hits; // verified, in offset order
+    uint64_t windows = 0;            // windows of the steps launched so far
+    uint64_t windows_collected = 0;  // windows of the steps collected: processed
+    std::vector<uint32_t> blocks;    // slot blocks held, in lane order
+    uint32_t lanes_last = 0;         // lanes held in the last step launched
+    uint32_t lanes_stride = 0;       // lane count the descriptor's stride is for
+    std::vector<og_batch_hit> hits;  // verified, in offset order
     bool done = false;
+    uint32_t status = OG_OK;         // OG_E_VERIFY when a device hit did not re-derive
     uint64_t admit_order = 0;
+};
+
+// The searches a launched step runs, as planned at its launch.
+struct Planned {
+    uint64_t id;
+    uint32_t sidx;
+    uint32_t half;
+    uint32_t lanes;
+    bool skippable;     // the device skips it once its quota is counted
+    uint64_t windows0;  // its W_done when the step starts
+};
+
+// One step's buffers: what the device writes while a newer step may already
+// be running, and the host staging of what the step's launch uploaded.
+struct Flight {
+    DevBuf<Counters> counters;
+    DevBuf<HitRec> surv, hits;
+    HostBuf<Counters> h_counters;
+    HostBuf<BatchDesc> h_descs;   // descriptors uploaded at this launch
+    HostBuf<SlotBlock> h_blocks;  // the block table this step ran (decodes its records)
+    HostBuf<uint32_t> h_init;     // init list, then its length at [nblocks]
+    HostBuf<SearchPos> h_pos;
+    BatchArgs args{};
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool pending = false;
+    std::vector<Planned> plan;
+
+    ~Flight() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+    }
 };
 
 }  // namespace
@@ -244,56 +345,59 @@ using namespace og;
 
 struct og_batch {
     int device = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaStream_t stream = nullptr;   // the steps
+    cudaStream_t ustream = nullptr;  // uploads of admitted searches' tables
+    cudaStream_t cstream = nullptr;  // a collected step's hits, while the next step runs
+    cudaMemPool_t pool = nullptr;
     og_batch_config cfg{};
     uint32_t slots = 0, nblocks = 0, grid = 0;
-    size_t smem = 0;
-    DevBuf<uint4> lanes, scratch, table, pow2;
+    DevBuf<uint4> lanes, scratch, table, pow8;
+    std::map<uint32_t, DevBuf<uint4>> pow2;  // per half
     DevBuf<BatchDesc> descs;
     DevBuf<SearchPos> pos;
-    HostBuf<SearchPos> h_pos;
-    DevBuf<uint4> pow8;
-    uint32_t suffix_searches = 0;  // admitted searches with suffixes
     DevBuf<SlotBlock> blocks;
     DevBuf<uint32_t> init_list;
-    DevBuf<Counters> counters;
-    DevBuf<HitRec> surv, hits;
-    HostBuf<BatchDesc> h_descs;
-    HostBuf<SlotBlock> h_blocks;
-    HostBuf<uint32_t> h_init;
-    HostBuf<Counters> h_counters;
+    DevBuf<uint32_t> found, mism;
+    std::vector<BatchDesc> h_descs;     // the descriptors as the host has them
+    std::vector<SlotBlock> h_blocks;    // the block table as the host has it
     HostBuf<HitRec> h_hits;
+    HostBuf<uint32_t> h_mism;
+    Flight flights[FLIGHTS];
+    uint64_t launched = 0, collected = 0;
+    uint32_t suffix_searches = 0;  // admitted searches with suffixes
     std::map<uint64_t, std::unique_ptr<Search>> searches;
     std::vector<uint32_t> free_sidx;
     std::vector<uint32_t> free_blocks;
-    std::map<uint32_t, std::array<FeWords, 3>> strides;  // per lane count
+    std::map<std::pair<uint32_t, uint32_t>, std::array<FeWords, 3>> strides;  // per (lanes, half)
     uint64_t admitted = 0;
     uint64_t mem_used = 0, mem_budget = 0;
-    uint64_t mismatches = 0;
     bool active_changed = true;
+    bool closed = false;
+    std::string closed_why;
     float last_ms = 0;
     uint64_t last_candidates = 0;
     uint32_t last_launches = 0;
     uint32_t dirty_lo = NONE, dirty_hi = 0;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    BatchArgs args{};
+    std::set<uint64_t> planted;  // searches whose next hit is treated as not re-deriving (tests)
 
     ~og_batch() {
+        cudaSetDevice(device);
         if (stream) cudaStreamSynchronize(stream);
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        searches.clear();
+        if (ustream) cudaStreamSynchronize(ustream);
+        searches.clear();  // their tables go back to the pool in stream order
+        if (stream) cudaStreamSynchronize(stream);
         if (stream) cudaStreamDestroy(stream);
-        if (ev0) cudaEventDestroy(ev0);
-        if (ev1) cudaEventDestroy(ev1);
+        if (ustream) cudaStreamDestroy(ustream);
+        if (cstream) cudaStreamDestroy(cstream);
+        if (pool) cudaMemPoolDestroy(pool);
     }
 
     void mark(uint32_t sidx) {
         dirty_lo = std::min(dirty_lo, sidx);
         dirty_hi = std::max(dirty_hi, sidx + 1);
     }
+
+    uint32_t pending() const { return (uint32_t)(launched - collected); }
 };
 
 namespace {
@@ -306,24 +410,34 @@ namespace {
                         "%s: %s", #call, cuda_text(_e).c_str());                                 \
     } while (0)
 
-const std::array<FeWords, 3>& stride_for(og_batch* b, uint32_t lanes) {
-    auto it = b->strides.find(lanes);
+const std::array<FeWords, 3>& stride_for(og_batch* b, uint32_t lanes, uint32_t half) {
+    const auto key = std::make_pair(lanes, half);
+    auto it = b->strides.find(key);
     if (it != b->strides.end()) return it->second;
     F51 x, y;
-    pt_affine(base_mult_u64(8ULL * (2ULL * b->cfg.half + 1) * lanes), x, y);
+    pt_affine(base_mult_u64(8ULL * (2ULL * half + 1) * lanes), x, y);
     std::array<FeWords, 3> w{to_words(x), to_words(y), to_words(f_mul(x, y))};
-    return b->strides.emplace(lanes, w).first->second;
+    return b->strides.emplace(key, w).first->second;
 }
 
 // Window W's centre for search s: s * B + 8 (W (2 half + 1) + half + 1) B.
-Pt window_centre(const og_batch* b, const Search& s, uint64_t w) {
-    const uint64_t k = 8ULL * (w * (2ULL * b->cfg.half + 1) + b->cfg.half + 1);
+Pt window_centre(const Search& s, uint64_t w) {
+    const uint64_t k = 8ULL * (w * (2ULL * s.half + 1) + s.half + 1);
     return pt_add(s.start, base_mult_u64(k));
 }
 
 void release_blocks(og_batch* b, Search& s) {
     for (uint32_t blk : s.blocks) b->free_blocks.push_back(blk);
     s.blocks.clear();
+}
+
+// A search ends: done with its quota, or failed with `status`. Its lanes go
+// back to the pool at the next launch.
+void finish(og_batch* b, Search& s, uint32_t status) {
+    s.done = true;
+    s.status = status;
+    release_blocks(b, s);
+    b->active_changed = true;
 }
 
 // Shares the slot pool equally among unfinished searches (the earliest
@@ -359,9 +473,10 @@ void rebalance(og_batch* b, std::vector<uint32_t>& init) {
             b->free_blocks.pop_back();
         }
         if (s.blocks.size() > had) {
-            // the new lanes start on windows W_done + lane
-            const Pt c = window_centre(b, s, s.windows);
-            BatchDesc& d = b->h_descs.p[s.sidx];
+            // the new lanes start on windows W_done + lane, W_done counting
+            // the steps already launched
+            const Pt c = window_centre(s, s.windows);
+            BatchDesc& d = b->h_descs[s.sidx];
             d.bx = to_words(c.X);
             d.by = to_words(c.Y);
             d.bz = to_words(c.Z);
@@ -370,22 +485,244 @@ void rebalance(og_batch* b, std::vector<uint32_t>& init) {
             for (size_t j = had; j < s.blocks.size(); j++) init.push_back(s.blocks[j]);
         }
     }
-    // the block table
-    for (uint32_t i = 0; i < b->nblocks; i++) b->h_blocks.p[i] = SlotBlock{NONE, 0};
+    for (uint32_t i = 0; i < b->nblocks; i++) b->h_blocks[i] = SlotBlock{NONE, 0};
     for (Search* s : running)
-        for (size_t j = 0; j < s->blocks.size(); j++) b->h_blocks.p[s->blocks[j]] = SlotBlock{s->sidx, (uint32_t)(j * BLOCK)};
+        for (size_t j = 0; j < s->blocks.size(); j++) b->h_blocks[s->blocks[j]] = SlotBlock{s->sidx, (uint32_t)(j * BLOCK)};
 }
 
-int enqueue_step(og_batch* b, char* err, size_t errlen) {
-    CU(cudaMemsetAsync(b->counters.p, 0, offsetof(Counters, init_count), b->stream));
-    CU(cudaMemsetAsync(&b->counters.p->surv, 0, 3 * sizeof(uint32_t), b->stream));  // surv, hits, mismatch
-    batch_init_kernel<<<b->nblocks, BLOCK, 0, b->stream>>>(b->args);
+int enqueue_step(og_batch* b, const BatchArgs& a, char* err, size_t errlen) {
+    CU(cudaMemsetAsync(a.counters, 0, offsetof(Counters, init_count), b->stream));
+    CU(cudaMemsetAsync(&a.counters->surv, 0, 3 * sizeof(uint32_t), b->stream));  // surv, hits, mismatch
+    batch_init_kernel<<<b->nblocks, BLOCK, 0, b->stream>>>(a);
     CU(cudaGetLastError());
-    batch_search_kernel<<<b->grid, BLOCK, b->smem, b->stream>>>(b->args);
+    batch_search_kernel<<<b->grid, BLOCK, 0, b->stream>>>(a);
     CU(cudaGetLastError());
-    batch_exact_kernel<<<b->grid, 256, 0, b->stream>>>(b->args);
+    batch_exact_kernel<<<b->grid, 256, 0, b->stream>>>(a);
     CU(cudaGetLastError());
-    CU(cudaMemcpyAsync(b->h_counters.p, b->counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, b->stream));
+    return OG_OK;
+}
+
+// Marks the batch unusable after an error that leaves its results in doubt;
+// later calls fail with OG_E_STATE.
+int close_batch(og_batch* b, int rc, const char* err) {
+    b->closed = true;
+    b->closed_why = err ? err : "an earlier error";
+    return rc;
+}
+
+// Expected candidates until the quota: quota over the chance that a
+// candidate matches (the prefixes' exact probability, plus each suffix's
+// symbol sets).
+double expected_work(const Search& s) {
+    double p = s.has_prefixes ? s.fs.match_probability() : 0.0;
+    for (size_t j = 0; j < s.sfx.size(); j++) {
+        double q = 1.0;
+        for (uint32_t set : s.sfx.pattern(j).sets) q *= __builtin_popcount(set) / 32.0;
+        p += q;
+    }
+    return p > 0 ? (double)s.quota / p : INFINITY;
+}
+
+// The search's inversion batch: the batch's half, doubled (up to max_half)
+// while the search's expected work covers LONG_STEPS steps of the whole pool
+// at the doubled half. Results do not depend on it.
+uint32_t choose_half(const og_batch* b, const Search& s) {
+    uint32_t h = b->cfg.half;
+    const double work = expected_work(s);
+    while (2 * h <= b->cfg.max_half && work >= LONG_STEPS * (2.0 * (2 * h) + 1) * b->slots * b->cfg.rounds) h *= 2;
+    return h;
+}
+
+// Plans and launches one step on the next free flight; `launched` says
+// whether anything ran (nothing does when no search holds lanes).
+int launch(og_batch* b, bool& launched, char* err, size_t errlen) {
+    launched = false;
+    Flight& f = b->flights[b->launched % FLIGHTS];
+    if (f.pending) return fail(err, errlen, OG_E_STATE, "no free step buffers");
+    std::vector<uint32_t> init;
+    if (b->active_changed) {
+        rebalance(b, init);
+        b->active_changed = false;
+    }
+    f.plan.clear();
+    for (auto& kv : b->searches) {
+        Search& s = *kv.second;
+        if (s.done || s.blocks.empty()) continue;
+        const uint32_t lanes = (uint32_t)s.blocks.size() * BLOCK;
+        if (lanes != s.lanes_stride) {
+            const auto& w = stride_for(b, lanes, s.half);
+            BatchDesc& d = b->h_descs[s.sidx];
+            d.wx = w[0];
+            d.wy = w[1];
+            d.wt = w[2];
+            s.lanes_stride = lanes;
+            b->mark(s.sidx);
+        }
+        f.plan.push_back(Planned{s.id, s.sidx, s.half, lanes, b->h_descs[s.sidx].quota != 0, s.windows});
+    }
+    if (f.plan.empty()) return OG_OK;
+    if (b->dirty_lo < b->dirty_hi) {
+        const size_t lo = b->dirty_lo, m = b->dirty_hi - b->dirty_lo;
+        std::memcpy(f.h_descs.p, b->h_descs.data() + lo, m * sizeof(BatchDesc));
+        CU(cudaMemcpyAsync(b->descs.p + lo, f.h_descs.p, m * sizeof(BatchDesc), cudaMemcpyHostToDevice, b->stream));
+        b->dirty_lo = NONE;
+        b->dirty_hi = 0;
+    }
+    std::memcpy(f.h_blocks.p, b->h_blocks.data(), b->nblocks * sizeof(SlotBlock));
+    CU(cudaMemcpyAsync(b->blocks.p, f.h_blocks.p, b->nblocks * sizeof(SlotBlock), cudaMemcpyHostToDevice, b->stream));
+    if (b->suffix_searches) {
+        // where each search stands, for the device's offset decode of its
+        // suffix survivors
+        uint32_t top = 0;
+        for (const Planned& p : f.plan) {
+            f.h_pos.p[p.sidx] = SearchPos{p.windows0, p.lanes, 0};
+            top = std::max(top, p.sidx + 1);
+        }
+        CU(cudaMemcpyAsync(b->pos.p, f.h_pos.p, top * sizeof(SearchPos), cudaMemcpyHostToDevice, b->stream));
+    }
+    for (size_t i = 0; i < init.size(); i++) f.h_init.p[i] = init[i];
+    if (!init.empty())
+        CU(cudaMemcpyAsync(b->init_list.p, f.h_init.p, init.size() * 4, cudaMemcpyHostToDevice, b->stream));
+    f.h_init.p[b->nblocks] = (uint32_t)init.size();
+    CU(cudaMemcpyAsync(&f.counters.p->init_count, &f.h_init.p[b->nblocks], 4, cudaMemcpyHostToDevice, b->stream));
+    CU(cudaEventRecord(f.ev0, b->stream));
+    if (f.exec) {
+        CU(cudaGraphLaunch(f.exec, b->stream));
+    } else {
+        int rc = enqueue_step(b, f.args, err, errlen);
+        if (rc != OG_OK) return rc;
+        CU(cudaMemcpyAsync(f.h_counters.p, f.counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, b->stream));
+    }
+    CU(cudaEventRecord(f.ev1, b->stream));
+    for (const Planned& p : f.plan) {
+        Search& s = *b->searches[p.id];
+        s.windows += (uint64_t)b->cfg.rounds * p.lanes;
+        s.lanes_last = p.lanes;
+    }
+    f.pending = true;
+    b->launched++;
+    launched = true;
+    return OG_OK;
+}
+
+// Waits for the oldest step in flight and takes its results: decodes every
+// exact hit's offset from the step's own plan and block table, and verifies
+// each search's hits in offset order up to its quota.
+int collect(og_batch* b, og_batch_hit* out, size_t cap, size_t* n, char* err, size_t errlen) {
+    Flight& f = b->flights[b->collected % FLIGHTS];
+    CU(cudaEventSynchronize(f.ev1));
+    f.pending = false;
+    b->collected++;
+    cudaEventElapsedTime(&b->last_ms, f.ev0, f.ev1);
+    b->last_launches = 3;
+    const Counters c = *f.h_counters.p;
+    if (c.surv > f.args.surv_cap || c.hits > f.args.hit_cap)
+        return fail(err, errlen, OG_E_OVERFLOW, "a step produced %u survivors (room %u) and %u hits (room %u)", c.surv,
+                    f.args.surv_cap, c.hits, f.args.hit_cap);
+    if (c.mismatch) {
+        // which searches' suffix survivors did not recompute (counts so far)
+        CU(cudaMemcpyAsync(b->h_mism.p, b->mism.p, b->cfg.max_searches * 4, cudaMemcpyDeviceToHost, b->cstream));
+        CU(cudaStreamSynchronize(b->cstream));
+    }
+    // the exact hits, on the copy stream: the next step runs on the engine's
+    std::vector<HitRec> recs(c.hits);
+    const size_t chunk = b->h_hits.n;
+    for (size_t off = 0; off < c.hits; off += chunk) {
+        const size_t m = std::min<size_t>(chunk, c.hits - off);
+        CU(cudaMemcpyAsync(b->h_hits.p, f.hits.p + off, m * sizeof(HitRec), cudaMemcpyDeviceToHost, b->cstream));
+        CU(cudaStreamSynchronize(b->cstream));
+        std::memcpy(recs.data() + off, b->h_hits.p, m * sizeof(HitRec));
+    }
+    std::unordered_map<uint32_t, size_t> by_sidx;
+    for (size_t i = 0; i < f.plan.size(); i++) by_sidx[f.plan[i].sidx] = i;
+    std::vector<std::vector<og_batch_hit>> found(f.plan.size());
+    for (const HitRec& h : recs) {
+        const SlotBlock sb = f.h_blocks.p[h.lane / BLOCK];
+        if (sb.sidx != h.search) continue;
+        auto it = by_sidx.find(sb.sidx);
+        if (it == by_sidx.end()) continue;
+        const Planned& p = f.plan[it->second];
+        const uint64_t slots_per_window = 2ULL * p.half + 1;
+        const uint64_t lane = sb.lane0 + h.lane % BLOCK;
+        const uint64_t r = h.step / slots_per_window, i = h.step % slots_per_window;
+        const uint64_t w = p.windows0 + r * p.lanes + lane;
+        og_batch_hit o{};
+        o.search_id = p.id;
+        o.offset = 8 * (w * slots_per_window + 1 + i);
+        for (int k = 0; k < 8; k++)
+            for (int j = 0; j < 4; j++) o.packed[4 * k + j] = (uint8_t)(h.y[k] >> (8 * j));
+        o.filter = h.pad;
+        found[it->second].push_back(o);
+    }
+    size_t emitted = 0;
+    uint64_t candidates = 0;
+    uint32_t failed = 0;
+    for (size_t pi = 0; pi < f.plan.size(); pi++) {
+        const Planned& p = f.plan[pi];
+        auto sit = b->searches.find(p.id);
+        if (sit == b->searches.end()) continue;  // retired since its launch
+        Search& s = *sit->second;
+        if (s.done) {
+            // finished in an earlier step: the device skipped its blocks
+            // when it could count its quota, otherwise it ran them
+            if (!p.skippable) candidates += (uint64_t)b->cfg.rounds * p.lanes * (2ULL * p.half + 1);
+            continue;
+        }
+        candidates += (uint64_t)b->cfg.rounds * p.lanes * (2ULL * p.half + 1);
+        s.windows_collected = p.windows0 + (uint64_t)b->cfg.rounds * p.lanes;
+        if (c.mismatch && b->h_mism.p[p.sidx]) {
+            finish(b, s, OG_E_VERIFY);
+            failed++;
+            continue;
+        }
+        std::vector<og_batch_hit>& v = found[pi];
+        std::sort(v.begin(), v.end(), [](const og_batch_hit& x, const og_batch_hit& y) { return x.offset < y.offset; });
+        bool bad = false;
+        for (og_batch_hit& h : v) {
+            if (s.hits.size() >= s.quota) break;
+            const uint32_t np = s.has_prefixes ? (uint32_t)s.fs.size() : 0;
+            if (h.filter < np && s.long_filters) {
+                const long fi = s.fs.match_key(h.packed);
+                if (fi < 0) continue;
+                h.filter = (uint32_t)fi;
+            }
+            uint8_t pk[32];
+            if (check_hit_scalar(s.scalar, h.offset, h.packed, pk) != HitCheck::ok || b->planted.erase(s.id)) {
+                bad = true;
+                break;
+            }
+            std::memcpy(h.public_key, pk, 32);
+            if (h.filter < np) {
+                // filters longer than the key-only span are confirmed on the address
+                const PrefixFilter& pf = s.fs.filter(h.filter);
+                if (pf.needs_full_check() && !pf.matches_address(address(pk))) continue;
+            } else {
+                // a suffix is confirmed on the re-derived key's address
+                uint8_t addr[35];
+                address_bytes(pk, addr);
+                if (s.sfx.match_address(addr) != (long)(h.filter - np)) {
+                    bad = true;
+                    break;
+                }
+            }
+            s.hits.push_back(h);
+            if (out && emitted < cap) out[emitted] = h;
+            emitted++;
+        }
+        if (bad) {
+            finish(b, s, OG_E_VERIFY);
+            failed++;
+        } else if (s.hits.size() >= s.quota) {
+            finish(b, s, OG_OK);
+        }
+    }
+    b->last_candidates = candidates;
+    *n = out ? std::min(emitted, cap) : 0;
+    if (failed)
+        return fail(err, errlen, OG_E_VERIFY,
+                    "%u searches ended with OG_E_VERIFY: a device hit did not re-derive on the host (see their status)",
+                    failed);
+    if (out && emitted > cap) return fail(err, errlen, OG_E_CAPACITY, "%zu hits and room for %zu", emitted, cap);
     return OG_OK;
 }
 
@@ -413,17 +750,26 @@ int og_batch_new(int ordinal, const og_batch_config* cfgp, og_batch** out, char*
         }
     }
     if (cfg.half == 0) cfg.half = 256;
-    if (cfg.half > 2048) return fail(err, errlen, OG_E_ARG, "half %u > 2048", cfg.half);
+    if (cfg.half > MAX_HALF) return fail(err, errlen, OG_E_ARG, "half %u > %u", cfg.half, MAX_HALF);
+    if (cfg.max_half == 0) cfg.max_half = cfg.half;
+    if (cfg.max_half < cfg.half || cfg.max_half > MAX_HALF)
+        return fail(err, errlen, OG_E_ARG, "max_half %u outside half %u .. %u", cfg.max_half, cfg.half, MAX_HALF);
+    {
+        uint32_t h = cfg.half;
+        while (h < cfg.max_half) h *= 2;
+        if (h != cfg.max_half) return fail(err, errlen, OG_E_ARG, "max_half %u is not half %u times a power of two", cfg.max_half, cfg.half);
+    }
     if (cfg.rounds == 0) cfg.rounds = 1;
     if (cfg.max_searches == 0) cfg.max_searches = 4096;
     if (cfg.graph > 2) return fail(err, errlen, OG_E_ARG, "graph mode %u", cfg.graph);
+    if (cfg.inflight == 0) cfg.inflight = 2;
+    if (cfg.inflight > FLIGHTS) return fail(err, errlen, OG_E_ARG, "inflight %u (1 or %d)", cfg.inflight, FLIGHTS);
     CU(cudaSetDevice(ordinal));
     std::unique_ptr<og_batch> b(new (std::nothrow) og_batch());
     if (!b) return fail(err, errlen, OG_E_NOMEM, "host memory");
     b->device = ordinal;
-    b->smem = 0;
     int per_sm = 0, sms = 0;
-    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_search_kernel, BLOCK, b->smem));
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_search_kernel, BLOCK, 0));
     CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ordinal));
     const uint32_t fit = (uint32_t)std::max(1, per_sm);
     cfg.grid = cfg.grid == 0 ? fit : std::min(cfg.grid, fit);
@@ -432,90 +778,119 @@ int og_batch_new(int ordinal, const og_batch_config* cfgp, og_batch** out, char*
     cfg.slots = (cfg.slots + BLOCK - 1) / BLOCK * BLOCK;
     b->slots = cfg.slots;
     b->nblocks = cfg.slots / BLOCK;
-    const uint64_t per_step = (uint64_t)cfg.slots * (2ULL * cfg.half + 1) * cfg.rounds;
-    // survivors per step stay below MAX_OCCUPANCY of the candidates; four times that, at least 2^20
-    const uint64_t surv_cap = std::max<uint64_t>(1ULL << 20, (uint64_t)(4.0 * MAX_OCCUPANCY * (double)per_step));
-    if (surv_cap > 0xffffffffULL) return fail(err, errlen, OG_E_ARG, "a step of %llu candidates is too large", (unsigned long long)per_step);
+    const uint64_t per_step = (uint64_t)cfg.slots * (2ULL * cfg.max_half + 1) * cfg.rounds;
+    // survivors per step: at most MAX_OCCUPANCY of the candidates pass, a
+    // sum of independent draws; room for that mean plus eight standard
+    // deviations, at least 2^20
+    const double mean = MAX_OCCUPANCY * (double)per_step;
+    const uint64_t surv_cap = std::max<uint64_t>(1ULL << 20, (uint64_t)(mean + 8.0 * std::sqrt(mean) + 4096.0));
+    if (surv_cap > 0x7fffffffULL) return fail(err, errlen, OG_E_ARG, "a step of %llu candidates is too large", (unsigned long long)per_step);
     if (cfg.max_hits == 0) cfg.max_hits = (uint32_t)surv_cap;
     b->cfg = cfg;
 
     CU(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-    CU(cudaEventCreate(&b->ev0));
-    CU(cudaEventCreate(&b->ev1));
+    CU(cudaStreamCreateWithFlags(&b->ustream, cudaStreamNonBlocking));
+    CU(cudaStreamCreateWithFlags(&b->cstream, cudaStreamNonBlocking));
+    {
+        // per-search tables: a pool of the batch's own, which never makes an
+        // allocation wait for a step by adding a dependency of its own
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = ordinal;
+        CU(cudaMemPoolCreate(&b->pool, &props));
+        int no = 0;
+        CU(cudaMemPoolSetAttribute(b->pool, cudaMemPoolReuseAllowInternalDependencies, &no));
+    }
     const size_t S = cfg.slots;
     CU(b->lanes.alloc(S * 4));
     // the scratch of the persistent CTAs, not of every slot: a CTA uses it for
     // one block of slots at a time
-    CU(b->scratch.alloc((size_t)b->grid * BLOCK * (2 * (size_t)cfg.half + 2) * 4));
-    const std::vector<uint4>& tab = pair_table(cfg.half);
+    CU(b->scratch.alloc((size_t)b->grid * BLOCK * (2 * (size_t)cfg.max_half + 2) * 4));
+    const std::vector<uint4>& tab = pair_table(cfg.max_half);
     CU(b->table.alloc(tab.size()));
-    CU(cudaMemcpyAsync(b->table.p, tab.data(), tab.size() * sizeof(uint4), cudaMemcpyHostToDevice, b->stream));
-    std::vector<uint4> pw = pow2_table(base_mult_u64(8ULL * (2ULL * cfg.half + 1)), POW2_BITS);
-    CU(b->pow2.alloc(pw.size()));
-    CU(cudaMemcpyAsync(b->pow2.p, pw.data(), pw.size() * sizeof(uint4), cudaMemcpyHostToDevice, b->stream));
+    CU(cudaMemcpy(b->table.p, tab.data(), tab.size() * sizeof(uint4), cudaMemcpyHostToDevice));
+    for (uint32_t h = cfg.half; h <= cfg.max_half; h *= 2) {
+        std::vector<uint4> pw = pow2_table(base_mult_u64(8ULL * (2ULL * h + 1)), POW2_BITS);
+        DevBuf<uint4>& d = b->pow2[h];
+        CU(d.alloc(pw.size()));
+        CU(cudaMemcpy(d.p, pw.data(), pw.size() * sizeof(uint4), cudaMemcpyHostToDevice));
+    }
+    b->h_descs.assign(cfg.max_searches, BatchDesc{});
     CU(b->descs.alloc(cfg.max_searches));
-    CU(b->h_descs.alloc(cfg.max_searches));
-    std::memset(b->h_descs.p, 0, cfg.max_searches * sizeof(BatchDesc));
     CU(b->pos.alloc(cfg.max_searches));
-    CU(b->h_pos.alloc(cfg.max_searches));
-    std::memset(b->h_pos.p, 0, cfg.max_searches * sizeof(SearchPos));
+    CU(b->found.alloc(cfg.max_searches));
+    CU(b->mism.alloc(cfg.max_searches));
+    CU(b->h_mism.alloc(cfg.max_searches));
+    CU(cudaMemset(b->found.p, 0, cfg.max_searches * 4));
+    CU(cudaMemset(b->mism.p, 0, cfg.max_searches * 4));
     std::vector<uint4> p8 = pow2_table(base_mult_u64(8), 64);
     CU(b->pow8.alloc(p8.size()));
-    CU(cudaMemcpyAsync(b->pow8.p, p8.data(), p8.size() * sizeof(uint4), cudaMemcpyHostToDevice, b->stream));
+    CU(cudaMemcpy(b->pow8.p, p8.data(), p8.size() * sizeof(uint4), cudaMemcpyHostToDevice));
     CU(b->blocks.alloc(b->nblocks));
-    CU(b->h_blocks.alloc(b->nblocks));
     CU(b->init_list.alloc(b->nblocks));
-    CU(b->h_init.alloc(b->nblocks + 1));
-    CU(b->counters.alloc(1));
-    CU(b->h_counters.alloc(1));
-    CU(b->surv.alloc(surv_cap));
-    CU(b->hits.alloc(cfg.max_hits));
     CU(b->h_hits.alloc(std::min<uint64_t>(cfg.max_hits, 1u << 16)));
-    for (uint32_t i = 0; i < b->nblocks; i++) {
-        b->h_blocks.p[i] = SlotBlock{NONE, 0};
-        b->free_blocks.push_back(b->nblocks - 1 - i);
-    }
+    b->h_blocks.assign(b->nblocks, SlotBlock{NONE, 0});
+    for (uint32_t i = 0; i < b->nblocks; i++) b->free_blocks.push_back(b->nblocks - 1 - i);
     for (uint32_t i = 0; i < cfg.max_searches; i++) b->free_sidx.push_back(cfg.max_searches - 1 - i);
-    CU(cudaMemcpyAsync(b->descs.p, b->h_descs.p, cfg.max_searches * sizeof(BatchDesc), cudaMemcpyHostToDevice, b->stream));
-    CU(cudaMemcpyAsync(b->blocks.p, b->h_blocks.p, b->nblocks * sizeof(SlotBlock), cudaMemcpyHostToDevice, b->stream));
-    CU(cudaStreamSynchronize(b->stream));
+    CU(cudaMemcpy(b->descs.p, b->h_descs.data(), cfg.max_searches * sizeof(BatchDesc), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(b->blocks.p, b->h_blocks.data(), b->nblocks * sizeof(SlotBlock), cudaMemcpyHostToDevice));
+
+    for (int fi = 0; fi < FLIGHTS; fi++) {
+        Flight& f = b->flights[fi];
+        CU(f.counters.alloc(1));
+        CU(cudaMemset(f.counters.p, 0, sizeof(Counters)));
+        CU(f.surv.alloc(surv_cap));
+        CU(f.hits.alloc(cfg.max_hits));
+        CU(f.h_counters.alloc(1));
+        CU(f.h_descs.alloc(cfg.max_searches));
+        CU(f.h_blocks.alloc(b->nblocks));
+        CU(f.h_init.alloc(b->nblocks + 1));
+        CU(f.h_pos.alloc(cfg.max_searches));
+        std::memset(f.h_pos.p, 0, cfg.max_searches * sizeof(SearchPos));
+        CU(cudaEventCreate(&f.ev0));
+        CU(cudaEventCreate(&f.ev1));
+        BatchArgs& a = f.args;
+        a.descs = b->descs.p;
+        a.blocks = b->blocks.p;
+        a.init_list = b->init_list.p;
+        a.counters = f.counters.p;
+        a.nblocks = b->nblocks;
+        a.lanes = b->lanes.p;
+        a.scratch = b->scratch.p;
+        a.slots = S;
+        a.table = b->table.p;
+        a.rounds = cfg.rounds;
+        a.surv = f.surv.p;
+        a.surv_cap = (uint32_t)surv_cap;
+        a.hits = f.hits.p;
+        a.hit_cap = cfg.max_hits;
+        a.pos = b->pos.p;
+        a.pow8 = b->pow8.p;
+        a.found = b->found.p;
+        a.mism = b->mism.p;
+        if (cfg.graph != 2) {
+            CU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+            int rc = enqueue_step(b.get(), a, err, errlen);
+            cudaError_t ce = rc == OG_OK ? cudaMemcpyAsync(f.h_counters.p, f.counters.p, sizeof(Counters),
+                                                           cudaMemcpyDeviceToHost, b->stream)
+                                         : cudaSuccess;
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+            if (rc != OG_OK) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            CU(ce);
+            CU(e);
+            f.graph = g;
+            CU(cudaGraphInstantiate(&f.exec, g, 0));
+        }
+    }
+    CU(cudaDeviceSynchronize());
     size_t free_b = 0, total_b = 0;
     CU(cudaMemGetInfo(&free_b, &total_b));
     b->mem_budget = cfg.memory_budget ? cfg.memory_budget : free_b / 2;
-
-    BatchArgs& a = b->args;
-    a.descs = b->descs.p;
-    a.blocks = b->blocks.p;
-    a.init_list = b->init_list.p;
-    a.counters = b->counters.p;
-    a.nblocks = b->nblocks;
-    a.lanes = b->lanes.p;
-    a.scratch = b->scratch.p;
-    a.slots = S;
-    a.table = b->table.p;
-    a.pow2 = b->pow2.p;
-    a.half = cfg.half;
-    a.rounds = cfg.rounds;
-    a.surv = b->surv.p;
-    a.surv_cap = (uint32_t)surv_cap;
-    a.hits = b->hits.p;
-    a.hit_cap = cfg.max_hits;
-    a.pos = b->pos.p;
-    a.pow8 = b->pow8.p;
-
-    if (cfg.graph != 2) {
-        CU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-        int rc = enqueue_step(b.get(), err, errlen);
-        cudaGraph_t g = nullptr;
-        cudaError_t e = cudaStreamEndCapture(b->stream, &g);
-        if (rc != OG_OK) {
-            if (g) cudaGraphDestroy(g);
-            return rc;
-        }
-        CU(e);
-        b->graph = g;
-        CU(cudaGraphInstantiate(&b->exec, g, 0));
-    }
     *out = b.release();
     return OG_OK;
 }
@@ -523,6 +898,7 @@ int og_batch_new(int ordinal, const og_batch_config* cfgp, og_batch** out, char*
 int og_batch_admit(og_batch* b, uint64_t search_id, const uint8_t seed[32], const char* filters, uint32_t quota,
                    char* err, size_t errlen) {
     if (!b || !seed || !filters) return fail(err, errlen, OG_E_ARG, "null argument");
+    if (b->closed) return fail(err, errlen, OG_E_STATE, "the batch is closed: %s", b->closed_why.c_str());
     if (quota == 0) return fail(err, errlen, OG_E_ARG, "a quota of zero");
     if (b->searches.count(search_id)) return fail(err, errlen, OG_E_STATE, "search %llu is already admitted", (unsigned long long)search_id);
     if (b->free_sidx.empty()) return fail(err, errlen, OG_E_CAPACITY, "%u searches are admitted already", b->cfg.max_searches);
@@ -552,9 +928,11 @@ int og_batch_admit(og_batch* b, uint64_t search_id, const uint8_t seed[32], cons
         return fail(err, errlen, OG_E_FILTER, "the filters leave %.1f%% of the index set (at most %.0f%% in a batch)",
                     100 * occupancy, 100 * MAX_OCCUPANCY);
     if (s->has_prefixes)
-        for (size_t i = 0; i < s->fs.size(); i++)
-            if (!s->fs.filter(i).is_pattern() && s->fs.filter(i).text.size() > FilterSet::DEVICE_SYMBOLS)
-            s->long_filters = true;
+        for (size_t i = 0; i < s->fs.size(); i++) {
+            const PrefixFilter& f = s->fs.filter(i);
+            if ((!f.is_pattern() && f.text.size() > FilterSet::DEVICE_SYMBOLS) || f.needs_full_check())
+                s->long_filters = true;
+        }
     std::vector<uint64_t> keys;
     std::vector<uint32_t> owners, pats;
     if (s->has_prefixes) {
@@ -576,32 +954,45 @@ int og_batch_admit(og_batch* b, uint64_t search_id, const uint8_t seed[32], cons
     if (b->mem_used + s->table_bytes > b->mem_budget)
         return fail(err, errlen, OG_E_NOMEM, "its tables (%llu bytes) do not fit the remaining budget (%llu of %llu used)",
                     (unsigned long long)s->table_bytes, (unsigned long long)b->mem_used, (unsigned long long)b->mem_budget);
+    s->half = choose_half(b, *s);
+    const auto pw = b->pow2.find(s->half);
+    if (pw == b->pow2.end() || !pw->second.p)
+        return fail(err, errlen, OG_E_STATE, "no lane-start table for half %u", s->half);
     CU(cudaSetDevice(b->device));
+    // the tables come from the batch's pool on the upload stream, so that
+    // nothing here waits for a step in flight
+    cudaStream_t u = b->ustream;
     if (s->has_prefixes) {
-        CU(s->bitmap.alloc(words32));
-        CU(s->keys.alloc(keys.size()));
-        CU(s->owners.alloc(owners.size()));
-        CU(cudaMemcpyAsync(s->bitmap.p, s->fs.words().data(), words32 * 4, cudaMemcpyHostToDevice, b->stream));
-        CU(cudaMemcpyAsync(s->keys.p, keys.data(), keys.size() * 8, cudaMemcpyHostToDevice, b->stream));
-        CU(cudaMemcpyAsync(s->owners.p, owners.data(), owners.size() * 4, cudaMemcpyHostToDevice, b->stream));
+        CU(s->bitmap.alloc(words32, b->pool, u, b->stream));
+        CU(s->keys.alloc(keys.size(), b->pool, u, b->stream));
+        CU(s->owners.alloc(owners.size(), b->pool, u, b->stream));
+        CU(cudaMemcpyAsync(s->bitmap.p, s->fs.words().data(), words32 * 4, cudaMemcpyHostToDevice, u));
+        if (!keys.empty()) CU(cudaMemcpyAsync(s->keys.p, keys.data(), keys.size() * 8, cudaMemcpyHostToDevice, u));
+        if (!owners.empty()) CU(cudaMemcpyAsync(s->owners.p, owners.data(), owners.size() * 4, cudaMemcpyHostToDevice, u));
         if (!pats.empty()) {
-            CU(s->patterns.alloc(pats.size()));
-            CU(cudaMemcpyAsync(s->patterns.p, pats.data(), pats.size() * 4, cudaMemcpyHostToDevice, b->stream));
+            CU(s->patterns.alloc(pats.size(), b->pool, u, b->stream));
+            CU(cudaMemcpyAsync(s->patterns.p, pats.data(), pats.size() * 4, cudaMemcpyHostToDevice, u));
         }
     }
     if (s->has_suffixes) {
-        CU(s->sbitmap.alloc(swords32));
-        CU(s->suffixes.alloc(rows.size()));
-        CU(cudaMemcpyAsync(s->sbitmap.p, s->sfx.words().data(), swords32 * 4, cudaMemcpyHostToDevice, b->stream));
-        CU(cudaMemcpyAsync(s->suffixes.p, rows.data(), rows.size() * 4, cudaMemcpyHostToDevice, b->stream));
+        CU(s->sbitmap.alloc(swords32, b->pool, u, b->stream));
+        CU(s->suffixes.alloc(rows.size(), b->pool, u, b->stream));
+        CU(cudaMemcpyAsync(s->sbitmap.p, s->sfx.words().data(), swords32 * 4, cudaMemcpyHostToDevice, u));
+        CU(cudaMemcpyAsync(s->suffixes.p, rows.data(), rows.size() * 4, cudaMemcpyHostToDevice, u));
     }
-    CU(cudaStreamSynchronize(b->stream));
+    // wait for the upload stream alone: the copies read pageable host memory,
+    // and once they are done any later step may read the tables
+    CU(cudaStreamSynchronize(u));
     s->sidx = b->free_sidx.back();
+    // its device counters start at zero, after every step launched so far
+    CU(cudaMemsetAsync(b->found.p + s->sidx, 0, 4, b->stream));
+    CU(cudaMemsetAsync(b->mism.p + s->sidx, 0, 4, b->stream));
     b->free_sidx.pop_back();
-    BatchDesc& d = b->h_descs.p[s->sidx];
+    BatchDesc& d = b->h_descs[s->sidx];
     std::memset(&d, 0, sizeof d);
     d.bitmap = s->bitmap.p;
     d.bits = s->fs.bits();
+    d.half = s->half;
     d.match = match_tables(s->buckets, s->keys.p, s->owners.p, s->patterns.p,
                            (uint32_t)(pats.size() / FilterSet::PATTERN_ROW));
     d.sbitmap = s->sbitmap.p;
@@ -609,6 +1000,10 @@ int og_batch_admit(og_batch* b, uint64_t search_id, const uint8_t seed[32], cons
     d.prefix_count = s->has_prefixes ? (uint32_t)s->fs.size() : 0;
     d.suffixes = s->suffixes.p;
     d.nsuffix = s->has_suffixes ? (uint32_t)s->sfx.size() : 0;
+    // the device may skip a search once it counts its quota, unless some of
+    // its hits still need the host's confirmation
+    d.quota = s->long_filters ? 0 : quota;
+    d.pow2 = pw->second.p;
     d.sx = to_words(s->start.X);
     d.sy = to_words(s->start.Y);
     d.sz = to_words(s->start.Z);
@@ -630,157 +1025,18 @@ int og_batch_step(og_batch* b, og_batch_hit* out, size_t cap, size_t* n, char* e
     b->last_ms = 0;
     b->last_candidates = 0;
     b->last_launches = 0;
+    if (b->closed) return fail(err, errlen, OG_E_STATE, "the batch is closed: %s", b->closed_why.c_str());
     CU(cudaSetDevice(b->device));
-    std::vector<uint32_t> init;
-    if (b->active_changed) {
-        rebalance(b, init);
-        b->active_changed = false;
+    while (b->pending() < b->cfg.inflight) {
+        bool launched = false;
+        const int rc = launch(b, launched, err, errlen);
+        if (rc != OG_OK) return close_batch(b, rc, err);
+        if (!launched) break;
     }
-    // strides for this step's lane counts
-    std::vector<Search*> sched;
-    for (auto& kv : b->searches) {
-        Search& s = *kv.second;
-        if (s.done || s.blocks.empty()) continue;
-        sched.push_back(&s);
-        const uint32_t lanes = (uint32_t)s.blocks.size() * BLOCK;
-        if (lanes != s.lanes_stride) {
-            const auto& w = stride_for(b, lanes);
-            BatchDesc& d = b->h_descs.p[s.sidx];
-            d.wx = w[0];
-            d.wy = w[1];
-            d.wt = w[2];
-            s.lanes_stride = lanes;
-            b->mark(s.sidx);
-        }
-    }
-    if (sched.empty()) return OG_OK;
-    if (b->dirty_lo < b->dirty_hi) {
-        CU(cudaMemcpyAsync(b->descs.p + b->dirty_lo, b->h_descs.p + b->dirty_lo,
-                           (b->dirty_hi - b->dirty_lo) * sizeof(BatchDesc), cudaMemcpyHostToDevice, b->stream));
-        b->dirty_lo = NONE;
-        b->dirty_hi = 0;
-    }
-    CU(cudaMemcpyAsync(b->blocks.p, b->h_blocks.p, b->nblocks * sizeof(SlotBlock), cudaMemcpyHostToDevice, b->stream));
-    if (b->suffix_searches) {
-        // where each search stands, for the device's offset decode of its
-        // suffix survivors
-        uint32_t top = 0;
-        for (Search* s : sched) {
-            b->h_pos.p[s->sidx] = SearchPos{s->windows, (uint32_t)s->blocks.size() * BLOCK, 0};
-            top = std::max(top, s->sidx + 1);
-        }
-        CU(cudaMemcpyAsync(b->pos.p, b->h_pos.p, top * sizeof(SearchPos), cudaMemcpyHostToDevice, b->stream));
-    }
-    for (size_t i = 0; i < init.size(); i++) b->h_init.p[i] = init[i];
-    if (!init.empty())
-        CU(cudaMemcpyAsync(b->init_list.p, b->h_init.p, init.size() * 4, cudaMemcpyHostToDevice, b->stream));
-    b->h_init.p[b->nblocks] = (uint32_t)init.size();
-    CU(cudaMemcpyAsync(&b->counters.p->init_count, &b->h_init.p[b->nblocks], 4, cudaMemcpyHostToDevice, b->stream));
-    CU(cudaEventRecord(b->ev0, b->stream));
-    if (b->exec) {
-        CU(cudaGraphLaunch(b->exec, b->stream));
-    } else {
-        int rc = enqueue_step(b, err, errlen);
-        if (rc != OG_OK) return rc;
-    }
-    CU(cudaEventRecord(b->ev1, b->stream));
-    CU(cudaStreamSynchronize(b->stream));
-    cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1);
-    b->last_launches = 3;
-    const Counters c = *b->h_counters.p;
-    if (c.surv > b->args.surv_cap || c.hits > b->args.hit_cap)
-        return fail(err, errlen, OG_E_OVERFLOW, "a step produced %u survivors (room %u) and %u hits (room %u)", c.surv,
-                    b->args.surv_cap, c.hits, b->args.hit_cap);
-    if (c.mismatch)
-        return fail(err, errlen, OG_E_VERIFY, "%u suffix survivors' keys recomputed from their offsets differ from "
-                    "the search kernel's", c.mismatch);
-    // copy the exact hits back in chunks
-    std::vector<HitRec> recs(c.hits);
-    const size_t chunk = b->h_hits.n;
-    for (size_t off = 0; off < c.hits; off += chunk) {
-        const size_t m = std::min<size_t>(chunk, c.hits - off);
-        CU(cudaMemcpyAsync(b->h_hits.p, b->hits.p + off, m * sizeof(HitRec), cudaMemcpyDeviceToHost, b->stream));
-        CU(cudaStreamSynchronize(b->stream));
-        std::memcpy(recs.data() + off, b->h_hits.p, m * sizeof(HitRec));
-    }
-    // decode offsets per search
-    const uint64_t slots_per_window = 2ULL * b->cfg.half + 1;
-    std::vector<Search*> by_sidx(b->cfg.max_searches, nullptr);
-    for (Search* s : sched) by_sidx[s->sidx] = s;
-    std::map<Search*, std::vector<og_batch_hit>> found;
-    for (const HitRec& h : recs) {
-        const uint32_t blk = h.lane / BLOCK;
-        const SlotBlock sb = b->h_blocks.p[blk];
-        Search* s = sb.sidx < by_sidx.size() ? by_sidx[sb.sidx] : nullptr;
-        if (!s || sb.sidx != h.search) continue;
-        const uint64_t lane = sb.lane0 + h.lane % BLOCK;
-        const uint64_t L = (uint64_t)s->blocks.size() * BLOCK;
-        const uint64_t r = h.step / slots_per_window, i = h.step % slots_per_window;
-        const uint64_t w = s->windows + r * L + lane;
-        og_batch_hit o{};
-        o.search_id = s->id;
-        o.offset = 8 * (w * slots_per_window + 1 + i);
-        for (int k = 0; k < 8; k++)
-            for (int j = 0; j < 4; j++) o.packed[4 * k + j] = (uint8_t)(h.y[k] >> (8 * j));
-        o.filter = h.pad;
-        found[s].push_back(o);
-    }
-    // advance, verify in offset order up to the quota
-    size_t emitted = 0;
-    uint64_t candidates = 0;
-    for (Search* s : sched) {
-        const uint64_t L = (uint64_t)s->blocks.size() * BLOCK;
-        s->lanes_last = (uint32_t)L;
-        s->windows += (uint64_t)b->cfg.rounds * L;
-        candidates += (uint64_t)b->cfg.rounds * L * slots_per_window;
-        auto it = found.find(s);
-        if (it == found.end()) continue;
-        std::vector<og_batch_hit>& v = it->second;
-        std::sort(v.begin(), v.end(), [](const og_batch_hit& x, const og_batch_hit& y) { return x.offset < y.offset; });
-        for (og_batch_hit& h : v) {
-            if (s->hits.size() >= s->quota) break;
-            const uint32_t np = s->has_prefixes ? (uint32_t)s->fs.size() : 0;
-            if (h.filter < np && s->long_filters) {
-                const long f = s->fs.match_key(h.packed);
-                if (f < 0) continue;
-                h.filter = (uint32_t)f;
-            }
-            uint8_t pk[32];
-            if (check_hit_scalar(s->scalar, h.offset, h.packed, pk) != HitCheck::ok) {
-                b->mismatches++;
-                continue;
-            }
-            std::memcpy(h.public_key, pk, 32);
-            if (h.filter < np) {
-                // filters longer than the key-only span are confirmed on the address
-                const PrefixFilter& f = s->fs.filter(h.filter);
-                if (f.needs_full_check() && !f.matches_address(address(pk))) continue;
-            } else {
-                // a suffix is confirmed on the re-derived key's address
-                uint8_t addr[35];
-                address_bytes(pk, addr);
-                if (s->sfx.match_address(addr) != (long)(h.filter - np)) {
-                    b->mismatches++;
-                    continue;
-                }
-            }
-            s->hits.push_back(h);
-            if (out && emitted < cap) out[emitted] = h;
-            emitted++;
-        }
-        if (s->hits.size() >= s->quota) {
-            s->done = true;
-            release_blocks(b, *s);
-            b->active_changed = true;
-        }
-    }
-    b->last_candidates = candidates;
-    *n = std::min(emitted, cap);
-    if (b->mismatches)
-        return fail(err, errlen, OG_E_VERIFY, "%llu device hits did not re-derive on the host",
-                    (unsigned long long)b->mismatches);
-    if (emitted > cap) return fail(err, errlen, OG_E_CAPACITY, "%zu hits and room for %zu", emitted, cap);
-    return OG_OK;
+    if (b->pending() == 0) return OG_OK;
+    const int rc = collect(b, out, cap, n, err, errlen);
+    if (rc != OG_OK && rc != OG_E_VERIFY && rc != OG_E_CAPACITY) return close_batch(b, rc, err);
+    return rc;
 }
 
 int og_batch_status(const og_batch* b, uint64_t search_id, og_search_status* st) {
@@ -788,14 +1044,16 @@ int og_batch_status(const og_batch* b, uint64_t search_id, og_search_status* st)
     auto it = b->searches.find(search_id);
     if (it == b->searches.end()) return OG_E_STATE;
     const Search& s = *it->second;
-    st->windows = s.windows;
-    st->candidates = s.windows * (2ULL * b->cfg.half + 1);
+    st->windows = s.windows_collected;
+    st->candidates = s.windows_collected * (2ULL * s.half + 1);
     st->hits = s.hits.size();
     st->lanes = s.lanes_last;
     st->quota = s.quota;
     st->done = s.done ? 1 : 0;
-    st->filters = (uint32_t)s.fs.size();
+    st->filters = (uint32_t)(s.fs.size() + s.sfx.size());
     st->table_bytes = s.table_bytes;
+    st->status = s.status;
+    st->half = s.half;
     return OG_OK;
 }
 
@@ -817,12 +1075,12 @@ int og_batch_retire(og_batch* b, uint64_t search_id) {
     if (it == b->searches.end()) return OG_E_STATE;
     Search& s = *it->second;
     cudaSetDevice(b->device);
-    cudaStreamSynchronize(b->stream);
     release_blocks(b, s);
     b->free_sidx.push_back(s.sidx);
     b->mem_used -= s.table_bytes;
     if (s.has_suffixes) b->suffix_searches--;
     if (!s.done) b->active_changed = true;
+    // its tables go back to the pool after the steps already launched
     b->searches.erase(it);
     return OG_OK;
 }
@@ -931,6 +1189,13 @@ int og_batch_tune(int ordinal, uint32_t searches, float max_step_ms, og_batch_co
     tuning_put(batch_key(ordinal), s);
     *out = best;
     if (keys_per_s) *keys_per_s = best_rate;
+    return OG_OK;
+}
+
+int og_batch_plant_mismatch(og_batch* b, uint64_t search_id) {
+    if (!b) return OG_E_ARG;
+    if (!b->searches.count(search_id)) return OG_E_STATE;
+    b->planted.insert(search_id);
     return OG_OK;
 }
 

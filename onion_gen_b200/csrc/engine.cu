@@ -211,15 +211,18 @@ namespace {
                         "%s: %s", #call, cuda_text(_e).c_str());                              \
     } while (0)
 
+// Lanes one wave of the search kernel holds: resident CTAs x block x lanes
+// per thread.
 int resident_lanes(int device, uint32_t scheme, uint32_t half, uint32_t block, uint32_t* out, char* err,
-                   size_t errlen) {
+                   size_t errlen, uint32_t lanes_per_thread = 1) {
     KernelInfo info{};
-    cudaError_t e = scheme == OG_SCHEME_CHAIN ? chain_info((int)block, &info) : paired_info((int)block, half, &info);
+    cudaError_t e = scheme == OG_SCHEME_CHAIN ? chain_info((int)block, &info)
+                                              : paired_info((int)block, half, lanes_per_thread, &info);
     if (e != cudaSuccess) return fail(err, errlen, OG_E_DEVICE, "kernel attributes: %s", cuda_text(e).c_str());
     int sms = 0;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return fail(err, errlen, OG_E_DEVICE, "device attributes: %s", cuda_text(e).c_str());
-    *out = (uint32_t)std::max(1, info.blocks_per_sm) * (uint32_t)sms * block;
+    *out = (uint32_t)std::max(1, info.blocks_per_sm) * (uint32_t)sms * block * lanes_per_thread;
     return OG_OK;
 }
 
@@ -269,6 +272,11 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
     if (cfg.block == 0) cfg.block = 128;
     if (cfg.block % 32 || cfg.block > OG_LB_THREADS)
         return fail(err, errlen, OG_E_ARG, "block %u (a multiple of 32, at most %d)", cfg.block, OG_LB_THREADS);
+    if (cfg.lanes_per_thread == 0) cfg.lanes_per_thread = 1;
+    if (cfg.lanes_per_thread > 2 || (cfg.scheme == OG_SCHEME_CHAIN && cfg.lanes_per_thread != 1))
+        return fail(err, errlen, OG_E_ARG, "%u lanes per thread (the paired scheme takes 1 or 2, the chain 1)",
+                    cfg.lanes_per_thread);
+    const uint32_t lpt = cfg.lanes_per_thread;
     const bool auto_half = cfg.half == 0;
     if (cfg.half == 0) cfg.half = cfg.scheme == OG_SCHEME_CHAIN ? 1024 : 2048;
     if (cfg.scheme == OG_SCHEME_PAIRED && cfg.half > 2048) return fail(err, errlen, OG_E_ARG, "half %u > 2048", cfg.half);
@@ -284,7 +292,7 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
     }
     if (cfg.lanes == 0) {
         uint32_t resident = 0;
-        int rc = resident_lanes(ordinal, cfg.scheme, cfg.half, cfg.block, &resident, err, errlen);
+        int rc = resident_lanes(ordinal, cfg.scheme, cfg.half, cfg.block, &resident, err, errlen, lpt);
         if (rc) return rc;
         if (cfg.scheme == OG_SCHEME_PAIRED) {
             // the persistent kernel takes lanes a block at a time: eight
@@ -309,7 +317,7 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
         }
     }
     const uint32_t slots = cfg.scheme == OG_SCHEME_CHAIN ? cfg.half : 2 * cfg.half + 1;
-    cfg.lanes = (cfg.lanes + cfg.block - 1) / cfg.block * cfg.block;
+    cfg.lanes = (cfg.lanes + cfg.block * lpt - 1) / (cfg.block * lpt) * (cfg.block * lpt);
     if (cfg.lanes > (1u << 24)) return fail(err, errlen, OG_E_ARG, "%u lanes (at most 2^24)", cfg.lanes);
     if (cfg.rounds == 0) {
         const uint64_t per_round = (uint64_t)cfg.lanes * slots;
@@ -349,11 +357,12 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
         // both kernels are persistent: scratch for the resident CTAs only
         // (the chain kernel's no more CTAs than blocks of lanes)
         uint32_t resident = 0;
-        int rc = resident_lanes(ordinal, cfg.scheme, cfg.half, cfg.block, &resident, err, errlen);
+        int rc = resident_lanes(ordinal, cfg.scheme, cfg.half, cfg.block, &resident, err, errlen, lpt);
         if (rc) return rc;
-        e->grid = std::max<uint32_t>(1, resident / cfg.block);
+        e->grid = std::max<uint32_t>(1, resident / (cfg.block * lpt));
         if (cfg.scheme == OG_SCHEME_CHAIN) e->grid = std::min<uint32_t>(e->grid, (uint32_t)(L / cfg.block));
-        CU(e->scratch.alloc((size_t)e->grid * cfg.block * elems * 4));
+        // one scratch column per lane a thread holds
+        CU(e->scratch.alloc((size_t)e->grid * cfg.block * lpt * elems * 4));
     }
     for (og_engine::Flight& f : e->fl) {
         CU(f.counts.alloc(4));
@@ -413,7 +422,8 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
         a.lanes = e->lanes.p;
         a.scratch = e->scratch.p;
         a.work = nullptr;  // the flight's counter, set per launch
-        a.slots_n = e->grid * cfg.block;
+        a.slots_n = e->grid * cfg.block * lpt;
+        a.lanes_per_thread = lpt;
         a.bitmap = cfg.dump ? nullptr : e->bitmap.p;
         a.bits = bits;
         a.sbitmap = e->sbitmap.p;
@@ -711,23 +721,28 @@ int og_engine_new(int ordinal, const uint8_t start[128], uint32_t threads, const
         cfg.lanes = shape.second;
         cfg.block = shape.block;
         cfg.rounds = shape.rounds;
+        cfg.lanes_per_thread = shape.lanes_per_thread;
         if (build_engine(ordinal, start, cfg, bitmap, words, bits, out, err, errlen) == OG_OK) return OG_OK;
         // the remembered shape no longer builds: measure again
     }
-    // Timed walk over inversion batch and lanes in flight; the fastest is
-    // kept and recorded (src/gpu/mod.rs:383-411).
+    // Timed walk over lanes per thread, inversion batch and lanes in flight
+    // (waves of the resident CTAs); the fastest is kept and recorded
+    // (src/gpu/mod.rs:383-411; the reference's OpenCL tuner walks two
+    // dimensions the same way, src/gpu/opencl.rs:207-271).
     og_engine* best = nullptr;
     double best_rate = -1;
     int last = OG_E_DEVICE;
+    for (uint32_t lpt : {1u, 2u})
     for (uint32_t half : {512u, 1024u, 2048u}) {
         uint32_t resident = 0;
-        if (resident_lanes(ordinal, OG_SCHEME_PAIRED, half, 128, &resident, err, errlen) != OG_OK) continue;
+        if (resident_lanes(ordinal, OG_SCHEME_PAIRED, half, 128, &resident, err, errlen, lpt) != OG_OK) continue;
         for (uint32_t mult : {2u, 4u, 8u}) {
             og_engine_config c{};
             c.scheme = OG_SCHEME_PAIRED;
             c.half = half;
             c.lanes = resident * mult;
             c.block = 128;
+            c.lanes_per_thread = lpt;
             og_engine* e = nullptr;
             last = build_engine(ordinal, start, c, bitmap, words, bits, &e, err, errlen);
             if (last != OG_OK) continue;
@@ -748,6 +763,7 @@ int og_engine_new(int ordinal, const uint8_t start[128], uint32_t threads, const
     s.second = best->cfg.lanes;
     s.block = best->cfg.block;
     s.rounds = best->cfg.rounds;
+    s.lanes_per_thread = best->cfg.lanes_per_thread;
     s.rate = best_rate;
     s.at = unix_now();
     tuning_put(key, s);

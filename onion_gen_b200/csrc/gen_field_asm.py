@@ -150,6 +150,54 @@ def reduce_tail():
     return L
 
 
+def reduce_tail_fold16():
+    """t0..t15 -> %0..%7 with 2^256 = 38, the high words folded by 16-bit
+    halves: t = h 2^16 + l gives 38 t = 38 l + (38 h) 2^16, where 38 l and
+    38 h are below 2^22 (narrow multiplies, no 64-bit result), and the byte
+    permutes split (38 h) 2^16 into (38 h) << 16, added to its own word, and
+    (38 h) >> 16, below 2^6, added to the next word. No wide multiply-add."""
+    L = []
+    for k in range(8):
+        t = f"t{8 + k}"
+        L.append(f"and.b32 l{k}, {t}, 65535;")
+        L.append(f"prmt.b32 h{k}, {t}, 0, 17458;")  # 0x4432: t >> 16
+        L.append(f"mul.lo.u32 l{k}, l{k}, 38;")
+        L.append(f"mul.lo.u32 h{k}, h{k}, 38;")
+    for k in range(8):
+        L.append(f"prmt.b32 x{k}, h{k}, 0, 4164;")  # 0x1044: (38 h) << 16
+        L.append(f"prmt.b32 y{k}, h{k}, 0, 17458;")  # (38 h) >> 16
+    # the small addends of each word: 38 l_k plus the spill of word k - 1
+    L.append("mov.u32 s0, l0;")
+    for k in range(1, 8):
+        L.append(f"add.u32 s{k}, l{k}, y{k - 1};")
+    L.append("add.cc.u32 r0, t0, x0;")
+    for k in range(1, 8):
+        L.append(f"addc.cc.u32 r{k}, t{k}, x{k};")
+    L.append("addc.u32 r8, y7, 0;")
+    L.append("add.cc.u32 r0, r0, s0;")
+    for k in range(1, 8):
+        L.append(f"addc.cc.u32 r{k}, r{k}, s{k};")
+    L.append("addc.u32 r8, r8, 0;")
+    # value = r0..r7 + r8 * 2^256 with r8 < 66: fold once more
+    L.append("mad.lo.cc.u32 r0, r8, 38, r0;")
+    for k in range(1, 8):
+        L.append(f"addc.cc.u32 r{k}, r{k}, 0;")
+    L.append("addc.u32 r8, 0, 0;")
+    # a carry here leaves r0..r7 below 38*66, so this add cannot carry
+    L.append("mad.lo.u32 r0, r8, 38, r0;")
+    for k in range(8):
+        L.append(f"mov.u32 %{k}, r{k};")
+    return L
+
+
+FOLD16 = "--fold16" in sys.argv
+TAIL_REGS = "\\n\\t.reg .u32 l<8>;\\n\\t.reg .u32 h<8>;\\n\\t.reg .u32 x<8>;\\n\\t.reg .u32 y<8>;\\n\\t.reg .u32 s<8>;"
+
+
+def tail():
+    return reduce_tail_fold16() if FOLD16 else reduce_tail()
+
+
 def emit_fn(name, body, nin, extra=""):
     out = []
     ins = ", ".join(f'"r"(a[{i}])' for i in range(8))
@@ -161,8 +209,9 @@ def emit_fn(name, body, nin, extra=""):
         else "const uint32_t* __restrict__ a"
     )
     out.append(f"__device__ __forceinline__ void {name}(uint32_t* __restrict__ r, {sig}) {{")
-    out.append('    asm("{\\n\\t.reg .u32 t<17>;\\n\\t.reg .u32 o<17>;\\n\\t.reg .u32 r<9>;\\n\\t' + extra + '"')
-    for line in body + reduce_tail():
+    regs = TAIL_REGS if FOLD16 else ""
+    out.append('    asm("{\\n\\t.reg .u32 t<17>;\\n\\t.reg .u32 o<17>;\\n\\t.reg .u32 r<9>;' + regs + '\\n\\t' + extra + '"')
+    for line in body + tail():
         out.append(f'        "{line}\\n\\t"')
     out.append('        "}"')
     outs = ", ".join(f'"=r"(r[{i}])' for i in range(8))
@@ -249,6 +298,14 @@ def simulate(lines, args):
             res = (-val(ops[1])) & M32
         elif base == "and":
             res = val(ops[1]) & val(ops[2])
+        elif base == "prmt":
+            src = val(ops[1]) | (val(ops[2]) << 32)
+            sel = val(ops[3])
+            res = 0
+            for i in range(4):
+                b = (sel >> (4 * i)) & 0xF
+                assert b < 8, "sign-replicating selectors are not used"
+                res |= ((src >> (8 * b)) & 0xFF) << (8 * i)
         elif base in ("sub", "subc"):
             d = val(ops[1]) - val(ops[2]) - (cc if base == "subc" else 0)
             res, borrow = d & M32, 1 if d < 0 else 0
@@ -272,8 +329,8 @@ def limbs(v):
 def check(n=20000):
     P = 2**255 - 19
     A, Bv = operands()
-    mul = mul_body(A, Bv) + reduce_tail()
-    sq = sq_body(A) + reduce_tail()
+    mul = mul_body(A, Bv) + tail()
+    sq = sq_body(A) + tail()
 
     rng = random.Random(1)
     special = [0, 1, 2**256 - 1, 2**255, 2**256 - 38, P, 2 * P, 2**255 - 1, 38]

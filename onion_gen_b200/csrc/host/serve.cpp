@@ -4,8 +4,10 @@
 // mutex; the worker admits from its head while the batch has room (it stops
 // at the first request the memory budget cannot take, so admission stays in
 // arrival order), runs a step, and completes every request whose quota is
-// met: its hits are copied out, its completion is stamped at the end of that
-// step, and it is retired so its lanes and tables go to the next requests.
+// met: its hits are copied out, its completion is stamped when that step's
+// results are taken, and it is retired so its lanes and tables go to the
+// next requests. The batch keeps a second step in flight meanwhile, so the
+// worker's admissions and completions overlap the device's work.
 #include <time.h>
 
 #include <algorithm>
@@ -55,7 +57,6 @@ struct og_serve {
     og_serve_stats stats{};                             // guarded by mu
     // worker-only state
     std::map<uint64_t, Request> running;
-    std::vector<og_batch_hit> stepbuf;
 
     void complete(const Request& r, uint32_t status, uint64_t candidates, std::vector<og_batch_hit>&& hits) {
         og_serve_done d{};
@@ -112,7 +113,9 @@ struct og_serve {
             if (running.empty()) continue;
             size_t n = 0;
             char err[256];
-            const int rc = og_batch_step(batch, stepbuf.data(), stepbuf.size(), &n, err, sizeof err);
+            // the step's hits stay in the batch; a request's come out of
+            // og_batch_results when it completes
+            const int rc = og_batch_step(batch, nullptr, 0, &n, err, sizeof err);
             const double ms = og_batch_last_step_ms(batch);
             const uint64_t cand = og_batch_last_step_candidates(batch);
             {
@@ -121,17 +124,21 @@ struct og_serve {
                 stats.candidates += cand;
                 stats.device_ms += ms;
             }
-            // collect finished requests (on a failed step every running request ends with its status)
+            // collect finished requests. A hit that did not re-derive
+            // (OG_E_VERIFY) ends only its own search, which completes with
+            // that status; any other failure closes the batch, and every
+            // running request ends with it.
+            const bool batch_failed = rc != OG_OK && rc != OG_E_VERIFY;
             std::vector<uint64_t> finished;
             for (auto& kv : running) {
                 og_search_status st;
                 if (og_batch_status(batch, kv.first, &st) != OG_OK) continue;
-                if (rc != OG_OK || st.done) {
+                if (batch_failed || st.done) {
                     std::vector<og_batch_hit> hits(st.quota);
                     size_t got = 0;
                     og_batch_results(batch, kv.first, hits.data(), hits.size(), &got);
                     hits.resize(got);
-                    complete(kv.second, rc == OG_OK ? OG_OK : (uint32_t)rc, st.candidates, std::move(hits));
+                    complete(kv.second, batch_failed ? (uint32_t)rc : st.status, st.candidates, std::move(hits));
                     finished.push_back(kv.first);
                 }
             }
@@ -162,7 +169,6 @@ int og_serve_new(int ordinal, const og_serve_config* cfg, og_serve** out, char* 
         return rc;
     }
     s->max_running = c.max_running ? c.max_running : (c.batch.max_searches ? c.batch.max_searches : 4096);
-    s->stepbuf.resize(og_batch_room(s->batch));
     s->worker = std::thread([s] { s->loop(); });
     *out = s;
     return OG_OK;

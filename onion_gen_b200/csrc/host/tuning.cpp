@@ -114,6 +114,7 @@ bool read_file(File& f) {
             else if (k == "at") s.at = std::strtoll(v.c_str(), nullptr, 10);
             else if (k == "block") s.block = (uint32_t)std::strtoul(v.c_str(), nullptr, 10);
             else if (k == "rounds") s.rounds = (uint32_t)std::strtoul(v.c_str(), nullptr, 10);
+            else if (k == "lanes_per_thread") s.lanes_per_thread = (uint32_t)std::strtoul(v.c_str(), nullptr, 10);
         }
     }
     return true;
@@ -174,6 +175,7 @@ void tuning_put(const std::string& key, const Shape& shape) {
           << "    at: " << s.at << "\n";
         if (s.block) o << "    block: " << s.block << "\n";
         if (s.rounds) o << "    rounds: " << s.rounds << "\n";
+        if (s.lanes_per_thread) o << "    lanes_per_thread: " << s.lanes_per_thread << "\n";
     }
     const size_t slash = path.rfind('/');
     if (slash != std::string::npos) mkdirs(path.substr(0, slash));

@@ -7,8 +7,8 @@
 // ~/.cache/onion-gen/ (src/tuning.rs:80-91) and written beside then renamed
 // (src/tuning.rs:103-125). For this engine `first` is the inversion batch
 // (`half`, a round being 2*half+1 candidates), `second` the lanes in flight;
-// `block` and `rounds` ride along as extra fields, which the reference's
-// reader ignores. Every failure is "no entry", never an error.
+// `block`, `rounds` and `lanes_per_thread` ride along as extra fields, which
+// the reference's reader ignores. Every failure is "no entry", never an error.
 #pragma once
 #include <cstdint>
 #include <string>
@@ -22,6 +22,7 @@ struct Shape {
     int64_t at = 0;
     uint32_t block = 0;
     uint32_t rounds = 0;
+    uint32_t lanes_per_thread = 0;
 };
 
 extern const char* const ENGINE_VERSION;

@@ -76,6 +76,47 @@ __global__ void __launch_bounds__(OG_LB_THREADS, OG_LB_MIN_BLOCKS) paired_kernel
     }
 }
 
+// Two lanes per thread (paired_rounds_n): each work item is 2 blocks of
+// lanes, thread t taking lanes item * 2 B + t and item * 2 B + B + t; the
+// scratch has two columns per thread, slot t and slot t + S / 2. Its
+// register bound (128 threads, OG_LB2_MIN_BLOCKS blocks per SM) holds the
+// two lanes' field elements without spills.
+#ifndef OG_LB2_MIN_BLOCKS
+#define OG_LB2_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(OG_LB_THREADS, OG_LB2_MIN_BLOCKS) paired_kernel2(const PairedArgs a) {
+    const uint4* qtab = a.table;
+    __shared__ uint32_t item_s;
+    const size_t L = a.lanes_n, S = a.slots_n;
+    const uint32_t per_item = 2 * blockDim.x;
+    const uint32_t nitems = a.lanes_n / per_item;
+    const uint32_t half_slots = a.slots_n / 2;
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    uint4* const scr[2] = {a.scratch + slot, a.scratch + half_slots + slot};
+    const Sink sink{a.bitmap, a.bits, a.hits, a.counter, a.cap, a.search, a.sbitmap, a.sbits};
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) item_s = atomicAdd(a.work, 1u);
+        __syncthreads();
+        const uint32_t item = item_s;
+        if (item >= nitems) break;
+        const uint32_t lane[2] = {item * per_item + threadIdx.x, item * per_item + blockDim.x + threadIdx.x};
+        fe x[2], y[2];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            x[k] = load_fe(a.lanes + 0 * L + lane[k], L);
+            y[k] = load_fe(a.lanes + 2 * L + lane[k], L);
+        }
+        paired_rounds_n<2>(x, y, words_fe(a.wx), words_fe(a.wy), words_fe(a.wt), qtab, a.half, a.rounds, scr, S,
+                           [&](int k, const fe& v, uint32_t step) { test_emit(sink, v, lane[k], step); });
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            store_fe(a.lanes + 0 * L + lane[k], L, x[k]);
+            store_fe(a.lanes + 2 * L + lane[k], L, y[k]);
+        }
+    }
+}
+
 // The chain kernel (the config-1 contract) keeps 96 registers: at 80 it
 // spills. Persistent like the paired kernel: each CTA takes the next block
 // of lanes until none is left, and the scratch is indexed by the CTA's
@@ -131,7 +172,9 @@ __device__ __noinline__ uint32_t suffix_owner(const MatchArgs& a, const HitRec& 
     const uint64_t w = a.window0 + (uint64_t)(r.step / a.slots) * a.lanes + r.lane;
     const uint64_t k = w * a.slots + (a.paired ? 1u : 0u) + r.step % a.slots;
     const SuffixTables t{a.suffixes, a.nsuffix, a.pow8};
-    const uint32_t j = suffix_match(t, a.sx, a.sy, a.sz, a.st, k, r.y, a.mismatch);
+    bool bad = false;
+    const uint32_t j = suffix_match(t, a.sx, a.sy, a.sz, a.st, k, r.y, bad);
+    if (bad) atomicAdd(a.mismatch, 1u);
     return j == 0xffffffffu ? j : a.prefix_count + j;
 }
 
@@ -174,9 +217,14 @@ cudaError_t launch_init(const InitArgs& a, int block, cudaStream_t s) {
 }
 
 cudaError_t launch_paired(const PairedArgs& a, int block, int grid, cudaStream_t s) {
-    if (a.lanes_n % block != 0 || block % 32 != 0 || grid <= 0 || a.slots_n != (uint32_t)grid * (uint32_t)block)
+    const uint32_t n = a.lanes_per_thread;
+    if ((n != 1 && n != 2) || block % 32 != 0 || grid <= 0 || a.lanes_n % ((uint32_t)block * n) != 0 ||
+        a.slots_n != (uint32_t)grid * (uint32_t)block * n)
         return cudaErrorInvalidValue;
-    paired_kernel<<<grid, block, 0, s>>>(a);
+    if (n == 2)
+        paired_kernel2<<<grid, block, 0, s>>>(a);
+    else
+        paired_kernel<<<grid, block, 0, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -197,8 +245,8 @@ static cudaError_t info_of(const void* fn, int block, size_t smem, KernelInfo* i
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&info->blocks_per_sm, fn, block, smem);
 }
 
-cudaError_t paired_info(int block, uint32_t, KernelInfo* info) {
-    return info_of((const void*)paired_kernel, block, 0, info);
+cudaError_t paired_info(int block, uint32_t, uint32_t lanes_per_thread, KernelInfo* info) {
+    return info_of(lanes_per_thread == 2 ? (const void*)paired_kernel2 : (const void*)paired_kernel, block, 0, info);
 }
 
 cudaError_t chain_info(int block, KernelInfo* info) { return info_of((const void*)chain_kernel, block, 0, info); }

@@ -59,9 +59,10 @@ struct PairedArgs {
     const uint32_t* sbitmap; // suffix bitmap (nullptr: none); with neither bitmap every candidate survives
     uint32_t sbits;
     FeWords wx, wy, wt;      // the round stride W = L (2 half + 1) 8 G, affine
-    uint32_t lanes_n;        // L, a multiple of the block size
+    uint32_t lanes_n;        // L, a multiple of the block size times lanes_per_thread
     uint32_t half;
     uint32_t rounds;         // rounds per launch
+    uint32_t lanes_per_thread;  // 1 (paired_kernel) or 2 (paired_kernel2); S = CTAs x block x this
 };
 
 struct ChainArgs {
@@ -150,8 +151,9 @@ struct MatchArgs {
 cudaError_t launch_init(const InitArgs& a, int block, cudaStream_t s);
 cudaError_t launch_match(const MatchArgs& a, int grid, cudaStream_t s);
 // The paired kernel is persistent: `grid` CTAs (the resident ones) take the
-// lanes a block at a time from `work`, so the scratch covers only the lanes
-// in flight and no SM idles in a tail wave.
+// lanes a block at a time (two blocks with two lanes per thread) from
+// `work`, so the scratch covers only the lanes in flight and no SM idles in
+// a tail wave.
 cudaError_t launch_paired(const PairedArgs& a, int block, int grid, cudaStream_t s);
 cudaError_t launch_chain(const ChainArgs& a, int block, int grid, cudaStream_t s);
 
@@ -163,7 +165,7 @@ struct KernelInfo {
     size_t local_bytes;
     int blocks_per_sm;
 };
-cudaError_t paired_info(int block, uint32_t half, KernelInfo* info);
+cudaError_t paired_info(int block, uint32_t half, uint32_t lanes_per_thread, KernelInfo* info);
 cudaError_t chain_info(int block, KernelInfo* info);
 
 }  // namespace og

@@ -256,4 +256,101 @@ __device__ __forceinline__ void paired_rounds(fe& x, fe& y, const fe& wx, const 
 #undef SCR
 }
 
+// N lanes per thread (N = 2): the rounds of paired_rounds for the lanes
+// (x[k], y[k]), k < N, whose scratch columns start at scr[k] (element e,
+// part w, half q at scr[k] + ((e * 2 + w) * 2 + q) * stride). The lanes'
+// passes are written step by step side by side, so that the scheduler can
+// issue one lane's products while the other lane's carry chains settle, and
+// the lanes of a thread share the table loads and one inversion per round
+// (Montgomery's trick over their N final products: 1 inversion and 3
+// multiplications instead of 2 inversions). `visit(k, y, step)` receives
+// lane k's candidates with the numbering of paired_rounds. Centres are
+// parked in shared memory as there (3 N field elements a thread).
+template <int N, class Visit>
+__device__ __forceinline__ void paired_rounds_n(fe (&x)[N], fe (&y)[N], const fe& wx, const fe& wy, const fe& wt,
+                                                const uint4* qtab, uint32_t half, uint32_t rounds,
+                                                uint4* const (&scr)[N], size_t stride, Visit&& visit) {
+    static_assert(N == 2, "paired_rounds covers one lane a thread; this function two");
+    const size_t L = stride;
+    const uint32_t slots = 2 * half + 1;
+    __shared__ uint4 park_s[N * 6 * PARK_STRIDE];
+    uint4* const park = park_s + threadIdx.x;
+#define SCRN(k, e, w) (scr[k] + ((size_t)(e) * 4 + (w) * 2) * L)
+    for (uint32_t r = 0; r < rounds; r++) {
+        fe run[N];
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+            const fe t = fe_mulv(x[k], y[k]);
+            const fe den0 = fe_sub(fe_mulv(x[k], wy), fe_mulv(y[k], wx));
+            store_fe(SCRN(k, 0, 0), L, fe_sub(t, wt));
+            store_fe(SCRN(k, 0, 1), L, den0);
+            const fe den1 = fe_sub(fe_mulv(y[k], wy), fe_mulv(x[k], wx));
+            store_fe(SCRN(k, 1, 0), L, fe_mulv(fe_add(t, wt), den0));
+            store_fe(SCRN(k, 1, 1), L, den1);
+            run[k] = fe_mulv(den0, den1);
+            park_fe(park, 3 * k + 0, x[k]);
+            park_fe(park, 3 * k + 1, y[k]);
+            park_fe(park, 3 * k + 2, t);
+        }
+#pragma unroll 1
+        for (uint32_t m = 1; m <= half; m++) {
+            const uint4* q = qtab + (size_t)(m - 1) * 6;
+            fe A[N], B[N];
+#pragma unroll
+            for (int k = 0; k < N; k++) {
+                A[k] = fe_mulv(unpark_fe(park, 3 * k + 0), load_fe(q + 2, 1));
+                B[k] = fe_mulv(unpark_fe(park, 3 * k + 1), load_fe(q + 0, 1));
+            }
+            const fe qt = load_fe(q + 4, 1);
+#pragma unroll
+            for (int k = 0; k < N; k++) {
+                const fe d0 = fe_sub(A[k], B[k]);  // P + Q_m
+                const fe tk = unpark_fe(park, 3 * k + 2);
+                store_fe(SCRN(k, 2 * m, 0), L, fe_mulv(fe_sub(tk, qt), run[k]));
+                store_fe(SCRN(k, 2 * m, 1), L, d0);
+                run[k] = fe_mulv(run[k], d0);
+                const fe d1 = fe_add(A[k], B[k]);  // P - Q_m
+                store_fe(SCRN(k, 2 * m + 1, 0), L, fe_mulv(fe_add(tk, qt), run[k]));
+                store_fe(SCRN(k, 2 * m + 1, 1), L, d1);
+                run[k] = fe_mulv(run[k], d1);
+            }
+        }
+        fe acc[N];
+        {
+            const fe inv = fe_invert(fe_mulv(run[0], run[1]));
+            acc[0] = fe_mulv(inv, run[1]);
+            acc[1] = fe_mulv(inv, run[0]);
+        }
+        const uint32_t base_step = r * slots;
+#pragma unroll
+        for (int k = 0; k < N; k++) visit(k, unpark_fe(park, 3 * k + 1), base_step + half);
+#pragma unroll 1
+        for (uint32_t m = half; m >= 1; m--) {
+            fe v[N];
+#pragma unroll
+            for (int k = 0; k < N; k++) {
+                v[k] = fe_mulv(load_fe(SCRN(k, 2 * m + 1, 0), L), acc[k]);
+                acc[k] = fe_mulv(acc[k], load_fe(SCRN(k, 2 * m + 1, 1), L));
+            }
+#pragma unroll
+            for (int k = 0; k < N; k++) visit(k, v[k], base_step + half - m);
+#pragma unroll
+            for (int k = 0; k < N; k++) {
+                v[k] = fe_mulv(load_fe(SCRN(k, 2 * m, 0), L), acc[k]);
+                acc[k] = fe_mulv(acc[k], load_fe(SCRN(k, 2 * m, 1), L));
+            }
+#pragma unroll
+            for (int k = 0; k < N; k++) visit(k, v[k], base_step + half + m);
+        }
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+            const fe xn = fe_mulv(load_fe(SCRN(k, 1, 0), L), acc[k]);
+            acc[k] = fe_mulv(acc[k], load_fe(SCRN(k, 1, 1), L));
+            y[k] = fe_mulv(load_fe(SCRN(k, 0, 0), L), acc[k]);
+            x[k] = xn;
+        }
+    }
+#undef SCRN
+}
+
 }  // namespace og

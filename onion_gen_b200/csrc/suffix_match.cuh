@@ -19,11 +19,11 @@ struct SuffixTables {
 // Index of the first suffix the key at scalar offset 8 k from `start`
 // matches, or 0xffffffff. The key is start + k 8G over the binary expansion
 // of k, made affine; its y must equal the survivor's canonical `yrec` (a
-// mismatch is counted in `mismatch` and never matched). The sign bit is the
-// parity of the canonical x.
+// mismatch sets `mismatch` and never matches; the caller counts it). The
+// sign bit is the parity of the canonical x.
 __device__ __forceinline__ uint32_t suffix_match(const SuffixTables& t, const FeWords& sx, const FeWords& sy,
                                                  const FeWords& sz, const FeWords& st, uint64_t k,
-                                                 const uint32_t yrec[8], uint32_t* mismatch) {
+                                                 const uint32_t yrec[8], bool& mismatch) {
     fe X = words_fe(sx), Y = words_fe(sy), Z = words_fe(sz), T = words_fe(st);
 #pragma unroll 1
     for (uint32_t j = 0; j < 64; j++)
@@ -36,10 +36,8 @@ __device__ __forceinline__ uint32_t suffix_match(const SuffixTables& t, const Fe
     bool same = true;
 #pragma unroll
     for (int q = 0; q < 8; q++) same &= y.v[q] == yrec[q];
-    if (!same) {
-        atomicAdd(mismatch, 1u);
-        return 0xffffffffu;
-    }
+    mismatch = !same;
+    if (!same) return 0xffffffffu;
     uint64_t pk[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) pk[q] = (uint64_t)y.v[2 * q] | ((uint64_t)y.v[2 * q + 1] << 32);

@@ -19,10 +19,10 @@ from .batch import _hit
 
 class Server:
     def __init__(self, device=0, half=0, slots=0, rounds=0, max_searches=0, max_hits=0, graph=True,
-                 memory_budget=0, max_running=0, grid=0):
+                 memory_budget=0, max_running=0, grid=0, max_half=0, inflight=0):
         ordinal = getattr(device, "ordinal", device)
         cfg = N.ServeConfig(N.BatchConfig(half, slots, rounds, max_searches, max_hits, 1 if graph else 2, grid,
-                                          memory_budget), max_running, 0)
+                                          memory_budget, max_half, inflight), max_running, 0)
         h = C.c_void_p()
         err = N.errbuf()
         N.check(N.lib.og_serve_new(int(ordinal), C.byref(cfg), C.byref(h), err, 512), err)

@@ -248,3 +248,86 @@ def test_a_lease_split_over_ranks_finds_the_same_hits(device):
     assert sorted(part) == [401]
     n = min(len(part[401]), len(whole[401]))
     assert n > 0 and part[401][:n] == whole[401][:n]
+
+
+def test_one_step_in_flight_agrees(device, mixed):
+    """With one step queued at a time (no overlap of host and device work)
+    the hits are the same as with two."""
+    out, _ = mixed
+    single, _ = run_batch(device, SEARCHES, inflight=1)
+    assert single == out
+
+
+def test_long_searches_at_a_larger_half_agree(device, mixed):
+    """max_half lets a search whose expected work covers four steps of the
+    whole pool run at a doubled inversion batch. Search 106 (one 5-symbol
+    prefix, quota 1) expects 2^25 = 3.355e7 candidates: four steps of 8192
+    slots at half 256 are 1.68e7, at half 512 3.358e7, so it runs at 256;
+    search 103 (200 4-symbol prefixes, quota 8) expects 4.2e4 and stays at
+    64. Their first hits do not change, nor do the others'."""
+    out, _ = mixed
+    b = B.Batch(device, **{**SMALL, "max_half": 512})
+    for sid, prefixes, quota in SEARCHES:
+        b.admit(sid, workloads.seed(sid), prefixes, quota)
+    halves = {sid: b.status(sid).half for sid, _, _ in SEARCHES}
+    assert halves[106] == 256 and halves[103] == 64, halves
+    steps = 0
+    while b.running():
+        b.step()
+        steps += 1
+        assert steps < 5000
+    got = {sid: [key_of(h) for h in b.results(sid)] for sid, _, _ in SEARCHES}
+    for sid, _, quota in SEARCHES:
+        st = b.status(sid)
+        assert st.done == 1 and st.hits == quota and st.status == 0
+        assert st.candidates == st.windows * (2 * halves[sid] + 1)
+    b.close()
+    assert got == out
+
+
+def test_overflow_closes_the_batch(device):
+    """More exact hits in a step than the room for them is an error, never
+    a truncation; the batch then refuses further steps and admissions."""
+    b = B.Batch(device, **{**SMALL, "max_hits": 4})
+    b.admit(1, workloads.seed(1), ["ab", "cd"], 16)  # about 2000 hits a step
+    with pytest.raises(N.OgError) as e:
+        for _ in range(4):
+            b.step()
+    assert e.value.status == "OG_E_OVERFLOW"
+    with pytest.raises(N.OgError) as e:
+        b.step()
+    assert e.value.status == "OG_E_STATE"
+    with pytest.raises(N.OgError) as e:
+        b.admit(2, workloads.seed(2), ["ab"], 1)
+    assert e.value.status == "OG_E_STATE"
+    b.close()
+
+
+def test_a_hit_that_does_not_rederive_ends_only_its_search(device, mixed):
+    """A re-derivation failure (planted on the host) ends that search with
+    OG_E_VERIFY for the step it happens in; the other searches go on and
+    find the same hits as in the mix without it, and later steps succeed."""
+    out, _ = mixed
+    b = B.Batch(device, **SMALL)
+    for sid, prefixes, quota in SEARCHES:
+        b.admit(sid, workloads.seed(sid), prefixes, quota)
+    b.plant_mismatch(105)
+    verify_errors = 0
+    steps = 0
+    while b.running():
+        try:
+            b.step()
+        except N.OgError as e:
+            assert e.status == "OG_E_VERIFY"
+            verify_errors += 1
+        steps += 1
+        assert steps < 5000
+    assert verify_errors == 1
+    st = b.status(105)
+    assert st.done == 1 and N.STATUS[st.status] == "OG_E_VERIFY" and st.hits < 16
+    for sid, _, quota in SEARCHES:
+        if sid == 105:
+            continue
+        assert b.status(sid).status == 0
+        assert [key_of(h) for h in b.results(sid)] == out[sid], sid
+    b.close()

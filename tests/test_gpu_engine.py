@@ -18,8 +18,8 @@ from onion_gen_b200 import gpu, key, workloads
 pytestmark = pytest.mark.gpu
 
 
-def cfg(scheme, half, lanes, rounds, dump=1, block=128, room=0):
-    return N.EngineConfig(scheme, half, lanes, rounds, block, dump, room)
+def cfg(scheme, half, lanes, rounds, dump=1, block=128, room=0, lanes_per_thread=0):
+    return N.EngineConfig(scheme, half, lanes, rounds, block, dump, room, lanes_per_thread)
 
 
 def oracle_start(oracle, seed):
@@ -79,6 +79,45 @@ def test_paired_consecutive_advances_tile_the_range(oracle, device, half, lanes,
     assert np.array_equal(offs, 8 * (1 + np.arange(n, dtype=np.uint64)))
     want = np.frombuffer(oracle.chain_keys_mt(start, 1, n), dtype=np.uint8).reshape(-1, 32)
     assert np.array_equal(keys, want)
+
+
+@pytest.mark.parametrize("half,lanes,rounds", [(32, 256, 3), (1, 256, 2), (300, 768, 1), (2048, 256, 1)])
+def test_two_lanes_per_thread_tile_the_range(oracle, device, half, lanes, rounds):
+    """The two-lanes-per-thread kernel (one inversion shared by a thread's
+    lanes) covers the same candidates bit for bit, advance after advance."""
+    start = oracle_start(oracle, workloads.seed(8))
+    eng = gpu.Engine(device, start, config=cfg(N.SCHEME_PAIRED, half, lanes, rounds, lanes_per_thread=2))
+    assert eng.shape().lanes_per_thread == 2
+    offs, keys = sorted_run(eng, advances=2)
+    n = 2 * lanes * (2 * half + 1) * rounds
+    assert np.array_equal(offs, 8 * (1 + np.arange(n, dtype=np.uint64)))
+    want = np.frombuffer(oracle.chain_keys_mt(start, 1, n), dtype=np.uint8).reshape(-1, 32)
+    assert np.array_equal(keys, want)
+
+
+def test_two_lanes_per_thread_filtered_equals_one(device):
+    """With a bitmap, the two kernels return the same survivors."""
+    fs = F.FilterSet.parse_all(["ab", "q7", "zz2"])
+    words, bits = fs.index_words()
+    start = key.start_point(workloads.seed(9))
+    got = []
+    for lpt in (1, 2):
+        eng = gpu.Engine(device, start, bitmap=words, bitmap_bits=bits,
+                         config=cfg(N.SCHEME_PAIRED, 256, 8192, 1, dump=0, lanes_per_thread=lpt))
+        offs, keys = sorted_run(eng, advances=2)
+        eng.close()
+        got.append((offs.tolist(), keys.tobytes()))
+    assert got[0] == got[1] and len(got[0][0]) > 1000
+
+
+def test_lanes_per_thread_is_checked(device):
+    start = key.start_point(workloads.seed(9))
+    with pytest.raises(N.OgError) as e:
+        gpu.Engine(device, start, config=cfg(N.SCHEME_PAIRED, 64, 256, 1, lanes_per_thread=3))
+    assert e.value.status == "OG_E_ARG"
+    with pytest.raises(N.OgError) as e:
+        gpu.Engine(device, start, config=cfg(N.SCHEME_CHAIN, 64, 256, 1, lanes_per_thread=2))
+    assert e.value.status == "OG_E_ARG"
 
 
 def test_chain_two_advances_continue(oracle, device):

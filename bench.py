@@ -73,12 +73,13 @@ SHORT_HALF = 256
 # the batch's shape comes from its autotuner, within this much device time a step
 BATCH_STEP_CAP_MS = 8.0
 CPU_HALF = 4096  # PairEngine::new(8192) (src/run.rs:601, src/batch.rs:32)
-# DRAM bytes per candidate of paired_kernel, from one ncu capture of one
-# launch at the plain line's shape (half 2048, 757,760 lanes on 740 persistent
-# CTAs: dram__bytes_read.sum + dram__bytes_write.sum = 198.88 + 198.85 GB for
-# 3,104,542,720 candidates); the algorithmic figure is 128 B (the Montgomery
-# scratch, 64 B written and 64 B read per candidate) whatever the shape.
-TRAFFIC_PER_CANDIDATE = 128.11
+# DRAM bytes per candidate of paired_kernel, from the ncu capture of the
+# small case (bench.py --case small: half 256, 757,760 lanes, one launch of
+# 388,730,880 candidates; dram__bytes_read.sum + dram__bytes_write.sum =
+# 24.96 + 25.03 GB), scaled to a launch of the plain line by its candidates:
+# the traffic is the Montgomery scratch, 64 B written and 64 B read per
+# candidate, whatever the shape, so it grows in proportion.
+TRAFFIC_PER_CANDIDATE = 128.6
 ALGORITHMIC_BYTES_PER_CANDIDATE = 128
 
 
@@ -90,11 +91,13 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--case", default="full", choices=["full", "small", "batch-small", "suffix-small", "chain-small"],
+    p.add_argument("--case", default="full",
+                   choices=["full", "small", "batch-small", "suffix-small", "chain-small", "config3-small"],
                    help="small: the profiling case, three one-round advances of the plain engine; "
                    "batch-small: three steps of the batched engine over the first 16 config-4 searches; "
                    "suffix-small: three advances of a forty-suffix search with the device match; "
-                   "chain-small: three advances of the chain scheme at its default shape")
+                   "chain-small: three advances of the chain scheme at its default shape; "
+                   "config3-small: three advances of config 3's 10,000-prefix search at its default shape")
     p.add_argument("--lanes-per-thread", type=int, default=1,
                    help="lanes each thread of the paired search kernel carries in --case small (1 or 2)")
     p.add_argument("--half", type=int, default=0,
@@ -497,23 +500,33 @@ def config3_leg(dev, peak, steps=2):
     batch = eng.batch()
     advances = -(-CANDIDATES_PER_STEP // batch)
     eng.advance_matches_raw()  # warm-up
+    # the matches land in the engine's own og_match buffer through the C
+    # ABI, as a caller in C takes them; only the sampled ones become Python
+    # objects
+    import ctypes as C
+
+    buf, room = eng._mbuf, eng.room()
     kernel_ms = 0.0
     matches = checked = 0
     rng = np.random.default_rng(3)
+    err = N.errbuf()
+    nout = C.c_size_t()
     t0 = time.perf_counter()
     total = steps * advances
     launched = 0
     for i in range(total):
         while launched - i < 2 and launched < total:
-            eng.launch_matches()
+            N.check(N.lib.og_engine_launch_matches(eng._h, err, 512), err)
             launched += 1
-        o, k, f = eng.collect_matches_raw()
+        N.check(N.lib.og_engine_collect_matches(eng._h, buf, room, C.byref(nout), err, 512), err)
         kernel_ms += eng.last_kernel_ms()
-        matches += len(o)
-        for j in rng.choice(len(o), size=min(64, len(o)), replace=False):
-            pk, _ = key.check_hit(seed, int(o[j]), bytes(k[j]))
-            if fs.match_address(pk) != int(f[j]):
-                raise RuntimeError(f"config 3: match at offset {int(o[j])} does not confirm on the host")
+        m = nout.value
+        matches += m
+        for j in rng.choice(m, size=min(64, m), replace=False):
+            h = buf[int(j)]
+            pk, _ = key.check_hit(seed, int(h.offset), bytes(h.packed))
+            if fs.match_address(pk) != int(h.filter):
+                raise RuntimeError(f"config 3: match at offset {int(h.offset)} does not confirm on the host")
             checked += 1
     wall = time.perf_counter() - t0
     eng.close()
@@ -533,6 +546,8 @@ def config3_leg(dev, peak, steps=2):
         "matches": matches,
         "match_fraction": matches / n,
         "matches_rederived": checked,
+        "e2e_note": "every match crosses to the host into the og_match buffer (48 bytes each, 5 % of the "
+        "candidates), with 64 of each advance's matches re-derived and confirmed on the host",
         "unit": "keys/s (CUDA events on the search kernel; e2e: wall clock with every match copied back)",
     }
 
@@ -607,6 +622,27 @@ def suffix_small_case(args):
     for i in range(3):
         o, _, _ = eng.advance_matches_raw()
         print(f"advance {i}: {len(o)} matches, search kernel {eng.last_kernel_ms():.3f} ms")
+
+
+def config3_small_case(args):
+    """Three advances of config 3's search (10,000 prefixes of 3..8 symbols,
+    a 24-bit index; 5 % of the candidates survive) at its default shape, or
+    --half: the case config 3's kernel summaries are captured on."""
+    from onion_gen_b200 import _native as N
+    from onion_gen_b200 import filter as F
+    from onion_gen_b200 import gpu, key, workloads
+
+    dev = gpu.look()[0]
+    fs = F.FilterSet.parse_all(workloads.config3_prefixes())
+    words, bits = fs.index_words()
+    eng = gpu.Engine(dev, key.start_point(workloads.seed(0)), bitmap=words, bitmap_bits=bits,
+                     config=N.EngineConfig(N.SCHEME_PAIRED, args.half, 0, 1, 128, 0, 0, args.lanes_per_thread))
+    shape = eng.shape()
+    for i in range(3):
+        o, _ = eng.advance_raw()
+        ms = eng.last_kernel_ms()
+        print(f"advance {i}: half {shape.half}, {shape.lanes} lanes, {bits}-bit index, {len(o)} survivors, "
+              f"kernel {ms:.3f} ms, {eng.batch() / ms * 1e3:.4e} keys/s")
 
 
 def chain_pp_per_candidate(n):
@@ -732,6 +768,9 @@ def main():
         return
     if args.case == "chain-small":
         chain_small_case(args)
+        return
+    if args.case == "config3-small":
+        config3_small_case(args)
         return
     rank, world, local = dist_env()
     import ctypes as C
@@ -905,7 +944,8 @@ def main():
                 "unit": "partial products/s",
                 "frac": achieved / peak,
                 "traffic": TRAFFIC_PER_CANDIDATE * batch,
-                "traffic_unit": "DRAM bytes per launch (ncu, dram__bytes_read.sum + dram__bytes_write.sum)",
+                "traffic_unit": "DRAM bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum on the "
+                "small case, 128.6 B a candidate, scaled to this launch's candidates)",
                 "per_candidate": w,
                 "peak_source": "measured: og_measure_int_peak mad.lo.u32 issue rate / 2 (lo+hi per product)",
                 "peak_theoretical": theoretical,

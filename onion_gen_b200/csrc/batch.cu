@@ -80,6 +80,9 @@ constexpr double MAX_OCCUPANCY = 0.02;
 // With max_half above half, a search runs at a doubled half while its
 // expected work covers at least this many steps of the whole pool there.
 constexpr double LONG_STEPS = 4.0;
+// A search needs the blocks that cover its expected remaining work in this
+// many steps.
+constexpr double NEED_STEPS = 2.0;
 
 struct BatchDesc {
     FeWords wx, wy, wt;      // the search's stride for this step: L (2 half + 1) 8 G, affine
@@ -285,6 +288,7 @@ struct Search {
     bool long_filters = false;  // some hit needs the host's confirmation beyond the device match
     uint32_t quota = 0;
     uint32_t half = 0;
+    double prob = 0;  // chance that a candidate matches one of its filters
     uint32_t sidx = NONE;
     PoolBuf<uint32_t> bitmap;
     PoolBuf<uint64_t> keys;
@@ -440,25 +444,72 @@ void finish(og_batch* b, Search& s, uint32_t status) {
     b->active_changed = true;
 }
 
-// Shares the slot pool equally among unfinished searches (the earliest
-// admitted first when there are more searches than blocks). Searches well
-// above their share drop their highest blocks; those below take free
-// blocks, whose lanes are queued for initialisation.
+// Shares the slot pool among unfinished searches by max-min fairness on
+// their needs: a search needs the blocks that cover its expected remaining
+// work ((quota - hits) over its match probability) in NEED_STEPS steps, at
+// least one. In ascending need (then admission order), each search gets its
+// need or an equal share of the blocks still unassigned, whichever is
+// smaller: short searches get all they can use and finish within a few
+// steps, long ones split the rest equally, and when there are more searches
+// than blocks the longest wait. Blocks nobody needs are spread evenly.
+// Searches well above their share drop their highest blocks; those below
+// take free blocks, whose lanes are queued for initialisation. Which lanes
+// a search holds never changes its results.
 void rebalance(og_batch* b, std::vector<uint32_t>& init) {
     std::vector<Search*> running;
     for (auto& kv : b->searches)
         if (!kv.second->done) running.push_back(kv.second.get());
-    std::sort(running.begin(), running.end(), [](Search* x, Search* y) { return x->admit_order < y->admit_order; });
-    const size_t n_sched = std::min<size_t>(running.size(), b->nblocks);
+    std::vector<double> need(running.size());
+    for (size_t i = 0; i < running.size(); i++) {
+        const Search& s = *running[i];
+        const double left = (double)(s.quota - std::min<size_t>(s.quota, s.hits.size()));
+        const double work = s.prob > 0 ? left / s.prob : INFINITY;
+        const double per_block = NEED_STEPS * (2.0 * s.half + 1) * b->cfg.rounds * BLOCK;
+        need[i] = std::max(1.0, std::ceil(work / per_block));
+    }
+    std::vector<size_t> order(running.size());
+    for (size_t i = 0; i < order.size(); i++) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](size_t x, size_t y) {
+        if (need[x] != need[y]) return need[x] < need[y];
+        return running[x]->admit_order < running[y]->admit_order;
+    });
+    {
+        std::vector<Search*> sorted(running.size());
+        std::vector<double> sneed(running.size());
+        for (size_t i = 0; i < order.size(); i++) {
+            sorted[i] = running[order[i]];
+            sneed[i] = need[order[i]];
+        }
+        running.swap(sorted);
+        need.swap(sneed);
+    }
     std::vector<uint32_t> target(running.size(), 0);
-    for (size_t i = 0; i < n_sched; i++)
-        target[i] = (uint32_t)(b->nblocks / n_sched + (i < b->nblocks % n_sched ? 1 : 0));
+    uint32_t left = b->nblocks;
+    for (size_t i = 0; i < running.size() && left; i++) {
+        const uint32_t share = left / (uint32_t)(running.size() - i);
+        target[i] = (uint32_t)std::min<double>(need[i], (double)share);
+        left -= target[i];
+    }
+    // blocks beyond every need: evenly over the searches that hold some
+    size_t held = 0;
+    for (uint32_t t : target) held += t ? 1 : 0;
+    for (size_t i = 0; i < running.size() && left && held; i++) {
+        if (!target[i]) continue;
+        const uint32_t extra = left / (uint32_t)held--;
+        target[i] += extra;
+        left -= extra;
+    }
     // Shrink only searches well above their share (a quarter over, at least
     // one block), so that arrivals and departures do not reshuffle every
     // search by a block each time; the free blocks go to those below it.
+    // While a search with a share holds no block at all, every search
+    // shrinks to its share exactly, so that a new arrival never waits for a
+    // departure.
+    bool starving = false;
+    for (size_t i = 0; i < running.size(); i++) starving |= target[i] > 0 && running[i]->blocks.empty();
     for (size_t i = 0; i < running.size(); i++) {
         Search& s = *running[i];
-        const size_t slack = target[i] ? std::max<size_t>(1, target[i] / 4) : 0;
+        const size_t slack = target[i] && !starving ? std::max<size_t>(1, target[i] / 4) : 0;
         if (s.blocks.size() <= target[i] + slack) continue;
         while (s.blocks.size() > target[i]) {
             b->free_blocks.push_back(s.blocks.back());
@@ -955,6 +1006,7 @@ int og_batch_admit(og_batch* b, uint64_t search_id, const uint8_t seed[32], cons
         return fail(err, errlen, OG_E_NOMEM, "its tables (%llu bytes) do not fit the remaining budget (%llu of %llu used)",
                     (unsigned long long)s->table_bytes, (unsigned long long)b->mem_used, (unsigned long long)b->mem_budget);
     s->half = choose_half(b, *s);
+    s->prob = (double)s->quota / expected_work(*s);
     const auto pw = b->pow2.find(s->half);
     if (pw == b->pow2.end() || !pw->second.p)
         return fail(err, errlen, OG_E_STATE, "no lane-start table for half %u", s->half);

@@ -302,16 +302,19 @@ def batch_shape(dev):
 LONG_SEARCH = 2e10
 
 
-def plain_arm(dev, searches, config):
+def plain_arm(dev, searches, config, device_match):
     """The run driver's loop (src/run.rs:1036-1074): one engine per search,
-    one search at a time, until its quota of verified hits."""
+    one search at a time, until its quota of verified hits; the survivors
+    are matched on the host (FilterSet::match_key, as the reference does)
+    or on the device."""
     from onion_gen_b200 import run
 
     out, examined, launches, per = {}, 0, 0, {}
     t0 = time.perf_counter()
     for s in searches:
         t1 = time.perf_counter()
-        found, ex, advances = run.device_search(dev, s.seed, s.prefixes, s.quota, config=config)
+        found, ex, advances = run.device_search(dev, s.seed, s.prefixes, s.quota, config=config,
+                                                device_match=device_match)
         per[s.index] = time.perf_counter() - t1
         out[s.index] = [(h.offset, h.packed) for h in found]
         examined += ex
@@ -344,12 +347,13 @@ def batched_leg(dev, shape, cap):
     probe.close()
     tuned_shape = {"half": tuned.half, "lanes": tuned.lanes, "rounds": tuned.rounds,
                    "candidates_per_advance": tuned.lanes * (2 * tuned.half + 1) * tuned.rounds}
-    plain_tuned, arm_tuned = plain_arm(dev, searches, None)
+    plain_tuned, arm_tuned = plain_arm(dev, searches, None, False)
     log(f"batched leg: plain engine (tuned shape {tuned_shape}) {len(searches)} searches in {arm_tuned['wall_s']:.2f} s")
     # the same loop with a short round (half 256, two waves of resident
-    # blocks: 9.7e7 candidates an advance), which overshoots a small quota less
+    # blocks: 9.7e7 candidates an advance), which overshoots a small quota
+    # less, and the exact match on the device, as the batch has it
     short = N.EngineConfig(N.SCHEME_PAIRED, SHORT_HALF, 2 * gpu.resident_lanes(dev), 1, 128, 0, 0)
-    plain_short, arm_short = plain_arm(dev, searches, short)
+    plain_short, arm_short = plain_arm(dev, searches, short, True)
     log(f"batched leg: plain engine (half {SHORT_HALF}) in {arm_short['wall_s']:.2f} s")
 
     t0 = time.perf_counter()
@@ -386,9 +390,11 @@ def batched_leg(dev, shape, cap):
         "expected_candidates": sum(s.expected_candidates() for s in searches),
         "candidates_to_quota": useful,
         "results_identical": plain_tuned == batched and plain_short == batched,
-        "plain_tuned": {"shape": tuned_shape, "constructor": "og_engine_new(threads = 0), the tuned shape", **arm_tuned},
+        "plain_tuned": {"shape": tuned_shape, "constructor": "og_engine_new(threads = 0), the tuned shape",
+                        "match": "host (FilterSet::match_key on every survivor, the reference's loop)", **arm_tuned},
         "plain_half256": {"shape": {"half": SHORT_HALF, "lanes": short.lanes, "rounds": 1},
-                          "constructor": "og_engine_new_config", **arm_short},
+                          "constructor": "og_engine_new_config", "match": "device (og_engine_match_on_device)",
+                          **arm_short},
         "batched": {"wall_s": batched_wall, "examined": examined, "keys_per_s": useful / batched_wall,
                     "examined_per_s": examined / batched_wall, "device_s": dev_ms / 1e3, "steps": steps,
                     "gpu_launches": launches, "halves": sorted(set(halves.values())),
@@ -737,14 +743,20 @@ def suffix_leg(dev, steps, advances):
 
 def batch_small_case(args):
     """Three steps of the batched engine with the first 16 config-4 searches
-    admitted: the case the batched kernels' ncu summaries are captured on."""
+    admitted (two of them long), at the batched leg's shape except for the
+    largest inversion batch: half 256, long searches at up to 512 (the leg
+    uses 2048; 512 keeps the scratch near 6 GB for a multi-pass capture), two
+    waves of slots, two steps in flight. The case the batched kernels' ncu
+    summaries are captured on."""
     from onion_gen_b200 import batch as B
     from onion_gen_b200 import gpu, workloads
 
     dev = gpu.look()[0]
-    b = B.Batch(dev, half=args.half or SHORT_HALF)
+    half = args.half or SHORT_HALF
+    b = B.Batch(dev, half=half, max_half=2 * half)
     for s in workloads.config4_searches()[:16]:
         b.admit(s.index, s.seed, s.prefixes, s.quota)
+    print("halves:", sorted(b.status(s.index).half for s in workloads.config4_searches()[:16]))
     for i in range(3):
         b.step()
         ms = b.last_step_ms()

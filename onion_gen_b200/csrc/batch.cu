@@ -784,12 +784,17 @@ extern "C" {
 int og_batch_new(int ordinal, const og_batch_config* cfgp, og_batch** out, char* err, size_t errlen) {
     if (!out) return fail(err, errlen, OG_E_ARG, "null argument");
     *out = nullptr;
+    og_batch_config cfg{};
+    if (cfgp) cfg = *cfgp;
+    // the fields that need no device first
+    if (cfg.half > MAX_HALF || cfg.max_half > MAX_HALF)
+        return fail(err, errlen, OG_E_ARG, "half %u / max_half %u (at most %u)", cfg.half, cfg.max_half, MAX_HALF);
+    if (cfg.graph > 2) return fail(err, errlen, OG_E_ARG, "graph mode %u", cfg.graph);
+    if (cfg.inflight > FLIGHTS) return fail(err, errlen, OG_E_ARG, "inflight %u (1 or %d)", cfg.inflight, FLIGHTS);
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
         return fail(err, errlen, OG_E_NODEVICE, "no CUDA device is available");
     if (ordinal < 0 || ordinal >= count) return fail(err, errlen, OG_E_ARG, "device %d of %d", ordinal, count);
-    og_batch_config cfg{};
-    if (cfgp) cfg = *cfgp;
     if (cfg.half == 0 && cfg.slots == 0 && cfg.rounds == 0 && cfg.grid == 0) {
         // the shape og_batch_tune recorded for this device, if any
         Shape s;

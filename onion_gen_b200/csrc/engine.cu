@@ -257,11 +257,14 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
         words = f->has_prefixes ? f->set.words().size() : 0;
         bits = f->has_prefixes ? f->set.bits() : 0;
     }
+    if (cfg.scheme > OG_SCHEME_CHAIN) return fail(err, errlen, OG_E_ARG, "unknown scheme %u", cfg.scheme);
+    if (cfg.lanes_per_thread > 2 || (cfg.scheme == OG_SCHEME_CHAIN && cfg.lanes_per_thread > 1))
+        return fail(err, errlen, OG_E_ARG, "%u lanes per thread (the paired scheme takes 1 or 2, the chain 1)",
+                    cfg.lanes_per_thread);
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
         return fail(err, errlen, OG_E_NODEVICE, "no CUDA device is available");
     if (ordinal < 0 || ordinal >= count) return fail(err, errlen, OG_E_ARG, "device %d of %d", ordinal, count);
-    if (cfg.scheme > OG_SCHEME_CHAIN) return fail(err, errlen, OG_E_ARG, "unknown scheme %u", cfg.scheme);
     if (!cfg.dump && (bitmap || !suffixed)) {
         if (!bitmap) return fail(err, errlen, OG_E_ARG, "no bitmap: without one every candidate would cross back");
         if (bits < 8 || bits > 32) return fail(err, errlen, OG_E_ARG, "bitmap width %u outside 8..32", bits);
@@ -273,9 +276,6 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
     if (cfg.block % 32 || cfg.block > OG_LB_THREADS)
         return fail(err, errlen, OG_E_ARG, "block %u (a multiple of 32, at most %d)", cfg.block, OG_LB_THREADS);
     if (cfg.lanes_per_thread == 0) cfg.lanes_per_thread = 1;
-    if (cfg.lanes_per_thread > 2 || (cfg.scheme == OG_SCHEME_CHAIN && cfg.lanes_per_thread != 1))
-        return fail(err, errlen, OG_E_ARG, "%u lanes per thread (the paired scheme takes 1 or 2, the chain 1)",
-                    cfg.lanes_per_thread);
     const uint32_t lpt = cfg.lanes_per_thread;
     const bool auto_half = cfg.half == 0;
     if (cfg.half == 0) cfg.half = cfg.scheme == OG_SCHEME_CHAIN ? 1024 : 2048;

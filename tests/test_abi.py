@@ -78,3 +78,22 @@ def test_product_does_not_reference_the_oracle():
     for path in glob.glob(os.path.join(ROOT, "onion_gen_b200", "**", "*"), recursive=True):
         if os.path.isfile(path) and path.endswith((".py", ".cu", ".cuh", ".cpp", ".h")):
             assert not pat.search(open(path, errors="replace").read()), path
+
+
+def test_batch_and_engine_shapes_are_checked_before_the_device(native, oracle):
+    """Shape fields that need no device are refused as OG_E_ARG whether or not
+    a device is present: the batch's half, max_half, inflight and graph mode,
+    and the engine's lanes per thread (1 or 2 for the paired scheme, 1 for
+    the chain)."""
+    N = native._native
+    err = N.errbuf()
+    h = ctypes.c_void_p()
+    for cfg in (N.BatchConfig(half=4096), N.BatchConfig(half=256, max_half=4096), N.BatchConfig(inflight=3),
+                N.BatchConfig(graph=3)):
+        rc = N.lib.og_batch_new(0, ctypes.byref(cfg), ctypes.byref(h), err, 512)
+        assert N.STATUS[rc] == "OG_E_ARG", err.value
+    start = oracle.scalar_base_mult(oracle.secret_scalar(bytes(32)))
+    for cfg in (N.EngineConfig(N.SCHEME_PAIRED, 64, 256, 1, 128, 1, 0, 3),
+                N.EngineConfig(N.SCHEME_CHAIN, 64, 256, 1, 128, 1, 0, 2)):
+        rc = N.lib.og_engine_new_config(0, start, ctypes.byref(cfg), None, 0, 0, ctypes.byref(h), err, 512)
+        assert N.STATUS[rc] == "OG_E_ARG", err.value

@@ -347,7 +347,7 @@ def batched_leg(dev, shape, cap):
     probe.close()
     tuned_shape = {"half": tuned.half, "lanes": tuned.lanes, "rounds": tuned.rounds,
                    "candidates_per_advance": tuned.lanes * (2 * tuned.half + 1) * tuned.rounds}
-    plain_tuned, arm_tuned = plain_arm(dev, searches, None, False)
+    plain_tuned, arm_tuned = plain_arm(dev, searches, None, True)
     log(f"batched leg: plain engine (tuned shape {tuned_shape}) {len(searches)} searches in {arm_tuned['wall_s']:.2f} s")
     # the same loop with a short round (half 256, two waves of resident
     # blocks: 9.7e7 candidates an advance), which overshoots a small quota
@@ -391,7 +391,7 @@ def batched_leg(dev, shape, cap):
         "candidates_to_quota": useful,
         "results_identical": plain_tuned == batched and plain_short == batched,
         "plain_tuned": {"shape": tuned_shape, "constructor": "og_engine_new(threads = 0), the tuned shape",
-                        "match": "host (FilterSet::match_key on every survivor, the reference's loop)", **arm_tuned},
+                        "match": "device (og_engine_match_on_device)", **arm_tuned},
         "plain_half256": {"shape": {"half": SHORT_HALF, "lanes": short.lanes, "rounds": 1},
                           "constructor": "og_engine_new_config", "match": "device (og_engine_match_on_device)",
                           **arm_short},

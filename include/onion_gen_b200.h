@@ -474,6 +474,11 @@ size_t og_filters_suffix_words(const og_filters* f, const uint64_t** words);
  * of the first match or -1. */
 long og_filters_match_address(const og_filters* f, const uint8_t pk[32]);
 double og_filters_occupancy(const og_filters* f);
+/* The chance that a uniform key matches some filter exactly: the prefixes'
+ * 32^-symbols (a pattern's set sizes over 32 per symbol) plus each suffix's,
+ * at most 1. The expected candidates to a hit are its inverse (the
+ * reference's estimate, src/estimate.rs, divides the same way). */
+double og_filters_match_probability(const og_filters* f);
 /* FilterSet::match_key (src/filter.rs:2098): index of the match or -1. */
 long og_filters_match(const og_filters* f, const uint8_t packed[32]);
 /* match_key over `n` keys laid out `stride` bytes apart (a survivor array's

@@ -203,6 +203,7 @@ def _load():
     sig("og_filters_bits", U32, [P])
     sig("og_filters_words", SZ, [P, C.POINTER(C.POINTER(U64))])
     sig("og_filters_occupancy", C.c_double, [P])
+    sig("og_filters_match_probability", C.c_double, [P])
     sig("og_filters_match", C.c_long, [P, B])
     sig("og_filters_match_many", SZ, [P, P, SZ, SZ, P])
     sig("og_filters_prefix_count", SZ, [P])

@@ -1,4 +1,5 @@
 // C ABI of the host side of the hit path: keys, re-derivation, filters.
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <string>
@@ -123,6 +124,18 @@ long og_filters_match_address(const og_filters* f, const uint8_t pk[32]) {
 }
 
 double og_filters_occupancy(const og_filters* f) { return f ? f->set.occupancy() : 0.0; }
+
+double og_filters_match_probability(const og_filters* f) {
+    if (!f) return 0.0;
+    double p = f->has_prefixes ? f->set.match_probability() : 0.0;
+    if (f->has_suffixes)
+        for (size_t j = 0; j < f->suffixes.size(); j++) {
+            double q = 1.0;
+            for (uint32_t set : f->suffixes.pattern(j).sets) q *= __builtin_popcount(set) / 32.0;
+            p += q;
+        }
+    return std::min(p, 1.0);
+}
 
 long og_filters_match(const og_filters* f, const uint8_t packed[32]) { return f ? f->set.match_key(packed) : -1; }
 

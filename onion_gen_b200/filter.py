@@ -60,6 +60,10 @@ class FilterSet:
     def occupancy(self) -> float:
         return N.lib.og_filters_occupancy(self._h)
 
+    def match_probability(self) -> float:
+        """The chance that a uniform key matches some filter exactly."""
+        return N.lib.og_filters_match_probability(self._h)
+
     def match_many(self, packed) -> np.ndarray:
         """match_key over an (n, 32) uint8 array: int32 indices, -1 where none matches."""
         arr = np.ascontiguousarray(packed, dtype=np.uint8)

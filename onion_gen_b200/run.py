@@ -50,12 +50,16 @@ def device_search(device, seed: bytes, prefixes, quota: int, threads: int = 0, c
     examined = 0
     launch = eng.launch_matches if device_match else eng.launch
     launched = 0
+    per_advance = eng.batch() * fs.match_probability()  # expected hits of one advance
     try:
         while len(found) < quota:
             if max_advances is not None and advances >= max_advances:
                 break
-            # keep the next advance running while this one is checked
-            while launched - advances < 2 and (max_advances is None or launched < max_advances):
+            # keep the next advance running while this one is checked, unless
+            # one advance is expected to bring four times the hits still
+            # needed: then the second would almost surely go unused
+            depth = 1 if per_advance >= 4 * (quota - len(found)) else 2
+            while launched - advances < depth and (max_advances is None or launched < max_advances):
                 launch()
                 launched += 1
             if device_match:

@@ -176,3 +176,18 @@ def test_rederivation_against_the_config1_sample(native):
         packed[31] &= 0x7F
         pk, _ = native.key.check_hit(seed, 8 * i, bytes(packed))
         assert pk.hex() == pub
+
+
+def test_match_probability(native):
+    """og_filters_match_probability: the kept prefixes' 32^-symbols (after
+    absorption), a pattern's set sizes over 32, and each suffix's."""
+    from onion_gen_b200 import workloads
+
+    F = native.filter
+    for s in workloads.config4_searches()[:12]:
+        fs = F.FilterSet.parse_all(s.prefixes)
+        assert abs(fs.match_probability() - s.match_probability()) <= 1e-12 * s.match_probability()
+    assert abs(F.FilterSet.parse_all(["ab", "abc", "q"]).match_probability() - (32.0 ** -2 + 32.0 ** -1)) < 1e-15
+    assert abs(F.FilterSet.parse_all(["a?", "[bc]d"]).match_probability() - (32.0 ** -1 + 2 * 32.0 ** -2)) < 1e-15
+    sfx = F.FilterSet.parse_all(["suffix:abcdefgad"])
+    assert abs(sfx.match_probability() - 32.0 ** -9) < 1e-20

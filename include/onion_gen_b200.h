@@ -474,10 +474,12 @@ size_t og_filters_suffix_words(const og_filters* f, const uint64_t** words);
  * of the first match or -1. */
 long og_filters_match_address(const og_filters* f, const uint8_t pk[32]);
 double og_filters_occupancy(const og_filters* f);
-/* The chance that a uniform key matches some filter exactly: the prefixes'
- * 32^-symbols (a pattern's set sizes over 32 per symbol) plus each suffix's,
- * at most 1. The expected candidates to a hit are its inverse (the
- * reference's estimate, src/estimate.rs, divides the same way). */
+/* FilterSet::probability (src/filter.rs:1979-1990): the chance that a
+ * uniform key's address matches some filter, 1 - prod(1 - p_f) over the kept
+ * filters, each p_f the product over its symbols of the accepted symbols the
+ * v3 protocol can produce there over those it can (src/filter.rs:226-238,
+ * 443-452). The expected candidates to a hit are its inverse
+ * (src/estimate.rs:69-78). */
 double og_filters_match_probability(const og_filters* f);
 /* FilterSet::match_key (src/filter.rs:2098): index of the match or -1. */
 long og_filters_match(const og_filters* f, const uint8_t packed[32]);

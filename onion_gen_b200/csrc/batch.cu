@@ -562,15 +562,12 @@ int close_batch(og_batch* b, int rc, const char* err) {
 }
 
 // Expected candidates until the quota: quota over the chance that a
-// candidate matches (the prefixes' exact probability, plus each suffix's
-// symbol sets).
+// candidate matches one of the search's filters (the reference's estimate,
+// src/estimate.rs:69-78, divides the same way).
 double expected_work(const Search& s) {
-    double p = s.has_prefixes ? s.fs.match_probability() : 0.0;
-    for (size_t j = 0; j < s.sfx.size(); j++) {
-        double q = 1.0;
-        for (uint32_t set : s.sfx.pattern(j).sets) q *= __builtin_popcount(set) / 32.0;
-        p += q;
-    }
+    std::vector<double> suffixes;
+    for (size_t j = 0; j < s.sfx.size(); j++) suffixes.push_back(s.sfx.pattern(j).probability());
+    const double p = either_of({s.has_prefixes ? s.fs.match_probability() : 0.0, either_of(suffixes)});
     return p > 0 ? (double)s.quota / p : INFINITY;
 }
 

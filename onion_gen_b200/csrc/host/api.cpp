@@ -127,14 +127,10 @@ double og_filters_occupancy(const og_filters* f) { return f ? f->set.occupancy()
 
 double og_filters_match_probability(const og_filters* f) {
     if (!f) return 0.0;
-    double p = f->has_prefixes ? f->set.match_probability() : 0.0;
-    if (f->has_suffixes)
-        for (size_t j = 0; j < f->suffixes.size(); j++) {
-            double q = 1.0;
-            for (uint32_t set : f->suffixes.pattern(j).sets) q *= __builtin_popcount(set) / 32.0;
-            p += q;
-        }
-    return std::min(p, 1.0);
+    std::vector<double> suffixes;
+    for (size_t j = 0; f->has_suffixes && j < f->suffixes.size(); j++) suffixes.push_back(f->suffixes.pattern(j).probability());
+    // the prefixes' and the suffixes' shares combine as the filters do
+    return og::either_of({f->has_prefixes ? f->set.match_probability() : 0.0, og::either_of(suffixes)});
 }
 
 long og_filters_match(const og_filters* f, const uint8_t packed[32]) { return f ? f->set.match_key(packed) : -1; }

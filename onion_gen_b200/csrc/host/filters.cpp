@@ -379,18 +379,20 @@ void FilterSet::device_patterns(std::vector<uint32_t>& rows) const {
 }
 
 double FilterSet::match_probability() const {
-    double p = 0;
+    // each kept filter anchored at the start, every symbol it names, the
+    // tail's protocol rooms included; combined as the reference does
+    std::vector<double> p;
+    p.reserve(filters_.size());
     for (const PrefixFilter& f : filters_) {
         if (f.is_pattern()) {
-            double q = 1;
-            for (size_t i = 0; i < std::min(f.sets.size(), KEY_ONLY_SYMBOLS); i++)
-                q *= __builtin_popcount(f.sets[i]) / 32.0;
-            p += q;
+            p.push_back(anchored_probability(f.sets.data(), f.sets.size(), 0));
         } else {
-            p += std::pow(32.0, -(double)std::min(f.text.size(), KEY_ONLY_SYMBOLS));
+            std::vector<uint32_t> sets(f.text.size());
+            for (size_t i = 0; i < f.text.size(); i++) sets[i] = 1u << base32_value(f.text[i]);
+            p.push_back(anchored_probability(sets.data(), sets.size(), 0));
         }
     }
-    return std::min(p, 1.0);
+    return either_of(p);
 }
 
 }  // namespace og

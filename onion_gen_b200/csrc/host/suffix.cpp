@@ -1,6 +1,7 @@
 #include "suffix.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 #include "keys.h"
@@ -159,6 +160,25 @@ bool parse_suffix(const std::string& raw, SuffixPattern& out, std::string& err) 
     out.sets = sets;
     out.text = render(sets);
     return true;
+}
+
+double anchored_probability(const uint32_t* sets, size_t n, size_t start) {
+    const uint32_t last = 1u << base32_value('d');
+    const uint32_t penultimate = (1u << base32_value('a')) | (1u << base32_value('i')) | (1u << base32_value('q')) |
+                                 (1u << base32_value('y'));
+    double p = 1.0;
+    for (size_t i = 0; i < n; i++) {
+        const size_t pos = start + i;
+        const uint32_t room = pos + 1 == ADDRESS_LEN ? last : pos + 2 == ADDRESS_LEN ? penultimate : ALL;
+        p *= (double)__builtin_popcount(sets[i] & room) / (double)__builtin_popcount(room);
+    }
+    return p;
+}
+
+double either_of(const std::vector<double>& p) {
+    double log_miss = 0.0;
+    for (double q : p) log_miss += std::log1p(-q);
+    return -std::expm1(log_miss);
 }
 
 bool SuffixSet::slots(const SuffixPattern& p, uint32_t bits, std::vector<uint32_t>& out) {

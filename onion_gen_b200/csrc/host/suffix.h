@@ -28,12 +28,22 @@ constexpr size_t SIGN_SYMBOL = 49;          // the symbol the sign bit (base32 b
 // string of `len` bytes; bits past the end read as zero.
 uint32_t symbol_at(const uint8_t* bytes, size_t len, size_t position);
 
+// The share of addresses whose symbols from `start` on fall in `sets`: per
+// position, the accepted symbols the protocol can produce there over the
+// symbols it can produce there (the last symbol is always 'd', the one
+// before it one of 'a', 'i', 'q', 'y'), multiplied over the positions
+// (Pattern::probability_at with protocol_allows, src/filter.rs:443-452,
+// 226-238).
+double anchored_probability(const uint32_t* sets, size_t n, size_t start);
+
 struct SuffixPattern {
     std::string text;             // canonical: "suffix:" + the body, lowercase
     std::vector<uint32_t> sets;   // bit v set = symbol value v allowed; position 56 - size() + i
     size_t start() const { return 56 - sets.size(); }
     // The exact check on the 35 bytes pk || checksum || version.
     bool matches_address(const uint8_t addr[35]) const;
+    // The share of addresses this suffix matches.
+    double probability() const { return anchored_probability(sets.data(), sets.size(), start()); }
     // The part a packed key (sign bit unknown) can decide: every position
     // below 51 the suffix reaches, with symbol 49 widened to both signs.
     bool key_prefilter(const uint8_t packed[32]) const;
@@ -74,6 +84,10 @@ private:
     std::vector<uint64_t> words_;
     uint32_t bits_ = 0;
 };
+
+// 1 - prod(1 - p) over a set's filters, kept small where p is (FilterSet::
+// probability, src/filter.rs:1979-1990, with log1p / expm1).
+double either_of(const std::vector<double>& p);
 
 // The 35 address bytes of a full public key: pk || checksum || 0x03.
 void address_bytes(const uint8_t pk[32], uint8_t out[35]);

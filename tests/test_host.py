@@ -1,6 +1,7 @@
 """The engine's host code through the C ABI, no GPU: keys, re-derivation,
 addresses, filters and the bitmap, against the golden fixtures and the oracle."""
 import json
+import math
 import os
 import random
 
@@ -178,16 +179,50 @@ def test_rederivation_against_the_config1_sample(native):
         assert pk.hex() == pub
 
 
+def _share(sets, start):
+    """Pattern::probability_at (src/filter.rs:443-452) with protocol_allows
+    (:226-238): per position, accepted and producible over producible."""
+    alphabet = "abcdefghijklmnopqrstuvwxyz234567"
+    p = 1.0
+    for i, want in enumerate(sets):
+        pos = start + i
+        room = {alphabet.index("d")} if pos == 55 else {alphabet.index(c) for c in "aiqy"} if pos == 54 else set(range(32))
+        p *= len(want & room) / len(room)
+    return p
+
+
+def _either(ps):
+    """FilterSet::probability (src/filter.rs:1979-1990): 1 - prod(1 - p)."""
+    return -math.expm1(sum(math.log1p(-p) for p in ps))
+
+
 def test_match_probability(native):
-    """og_filters_match_probability: the kept prefixes' 32^-symbols (after
-    absorption), a pattern's set sizes over 32, and each suffix's."""
+    """og_filters_match_probability restates the reference's FilterSet::
+    probability: each kept filter's share with the protocol's tail rooms,
+    combined as 1 - prod(1 - p)."""
     from onion_gen_b200 import workloads
 
     F = native.filter
+    alphabet = "abcdefghijklmnopqrstuvwxyz234567"
+
+    def lit(text):
+        return [{alphabet.index(c)} for c in text]
+
     for s in workloads.config4_searches()[:12]:
-        fs = F.FilterSet.parse_all(s.prefixes)
-        assert abs(fs.match_probability() - s.match_probability()) <= 1e-12 * s.match_probability()
-    assert abs(F.FilterSet.parse_all(["ab", "abc", "q"]).match_probability() - (32.0 ** -2 + 32.0 ** -1)) < 1e-15
-    assert abs(F.FilterSet.parse_all(["a?", "[bc]d"]).match_probability() - (32.0 ** -1 + 2 * 32.0 ** -2)) < 1e-15
+        kept = []
+        for p in sorted(set(s.prefixes)):
+            if not (kept and p.startswith(kept[-1])):
+                kept.append(p)
+        want = _either([_share(lit(p), 0) for p in kept])
+        assert math.isclose(F.FilterSet.parse_all(s.prefixes).match_probability(), want, rel_tol=1e-12)
+    # a pattern with a wildcard and a class
+    want = _either([_share([{alphabet.index("a")}, set(range(32))], 0), _share([{1, 2}, {3}], 0)])
+    assert math.isclose(F.FilterSet.parse_all(["a?", "[bc]d"]).match_probability(), want, rel_tol=1e-12)
+    # a suffix pays for its tail only where the protocol leaves a choice:
+    # 'd' last is free, 'a' before it one in four
     sfx = F.FilterSet.parse_all(["suffix:abcdefgad"])
-    assert abs(sfx.match_probability() - 32.0 ** -9) < 1e-20
+    assert math.isclose(sfx.match_probability(), 32.0 ** -7 / 4, rel_tol=1e-12)
+    assert math.isclose(sfx.match_probability(), _share(lit("abcdefgad"), 56 - 9), rel_tol=1e-12)
+    # prefixes and suffixes together
+    both = F.FilterSet.parse_all(["ab", "suffix:qqqqqqqid"])
+    assert math.isclose(both.match_probability(), _either([32.0 ** -2, 32.0 ** -7 / 4]), rel_tol=1e-12)

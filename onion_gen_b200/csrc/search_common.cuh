@@ -40,7 +40,14 @@ struct Sink {
     uint32_t search;
     const uint32_t* sbitmap;  // suffix bitmap, or nullptr
     uint32_t sbits;
+    // the prefix bitmap is read from the block's copy in shared memory
+    // (og_bitmap_s, staged by the kernel), not through L1
+    bool staged = false;
 };
+
+// Prefix bitmaps of at most this many bits (8 KiB) can be staged in shared
+// memory by a kernel that sets Sink::staged.
+constexpr uint32_t STAGED_BITMAP_BITS = 16;
 
 // Slot of a canonical key in the suffix bitmap: base32 bits
 // [255 - sbits, 255) of the packed key, i.e. bits 1..sbits of its last eight
@@ -78,7 +85,12 @@ __device__ __forceinline__ void test_emit(const Sink& k, const fe& yraw, uint32_
             // bytes 0..3 of the key, big-endian: the top of the slot
             const uint32_t head = __byte_perm(y.v[0], 0, 0x0123);
             const uint32_t slot = k.bits >= 32 ? head : head >> (32 - k.bits);
-            hit = (__ldg(k.bitmap + (slot >> 5)) >> (slot & 31)) & 1u;
+            if (k.staged) {
+                extern __shared__ uint32_t og_bitmap_s[];
+                hit = (og_bitmap_s[slot >> 5] >> (slot & 31)) & 1u;
+            } else {
+                hit = (__ldg(k.bitmap + (slot >> 5)) >> (slot & 31)) & 1u;
+            }
         }
         if (k.sbitmap) {
             const uint32_t slot = suffix_slot(y, k.sbits);

@@ -310,6 +310,7 @@ struct Search {
 // The searches a launched step runs, as planned at its launch.
 struct Planned {
     uint64_t id;
+    uint64_t admit_order;  // tells the search apart from a later one admitted under the same id
     uint32_t sidx;
     uint32_t half;
     uint32_t lanes;
@@ -606,7 +607,7 @@ int launch(og_batch* b, bool& launched, char* err, size_t errlen) {
             s.lanes_stride = lanes;
             b->mark(s.sidx);
         }
-        f.plan.push_back(Planned{s.id, s.sidx, s.half, lanes, b->h_descs[s.sidx].quota != 0, s.windows});
+        f.plan.push_back(Planned{s.id, s.admit_order, s.sidx, s.half, lanes, b->h_descs[s.sidx].quota != 0, s.windows});
     }
     if (f.plan.empty()) return OG_OK;
     if (b->dirty_lo < b->dirty_hi) {
@@ -708,7 +709,8 @@ int collect(og_batch* b, og_batch_hit* out, size_t cap, size_t* n, char* err, si
     for (size_t pi = 0; pi < f.plan.size(); pi++) {
         const Planned& p = f.plan[pi];
         auto sit = b->searches.find(p.id);
-        if (sit == b->searches.end()) continue;  // retired since its launch
+        // retired since its launch (and perhaps its id admitted again)
+        if (sit == b->searches.end() || sit->second->admit_order != p.admit_order) continue;
         Search& s = *sit->second;
         if (s.done) {
             // finished in an earlier step: the device skipped its blocks

@@ -331,3 +331,27 @@ def test_a_hit_that_does_not_rederive_ends_only_its_search(device, mixed):
         assert b.status(sid).status == 0
         assert [key_of(h) for h in b.results(sid)] == out[sid], sid
     b.close()
+
+
+def test_an_id_admitted_again_while_a_step_is_in_flight(device):
+    """A search retired while it holds lanes in the step still in flight, and
+    its id admitted again at once with other filters: the old search's hits
+    in that step are not taken for the new one's, whose result equals a
+    fresh run of it."""
+    b = B.Batch(device, **SMALL)
+    b.admit(5, workloads.seed(50), ["ab"], 50000)  # about 2000 hits a step, far from its quota
+    b.admit(6, workloads.seed(6), ["q7"], 2)
+    b.step()  # two steps launched, the first collected: search 5 has lanes in the second
+    assert b.status(5).done == 0
+    b.retire(5)
+    b.admit(5, workloads.seed(5), ["cd"], 3)
+    steps = 0
+    while b.running():
+        b.step()
+        steps += 1
+        assert steps < 5000
+    assert b.status(5).status == 0 and b.status(6).status == 0
+    got = [key_of(h) for h in b.results(5)]
+    b.close()
+    alone, _ = run_batch(device, [(5, ["cd"], 3)])
+    assert got == alone[5]

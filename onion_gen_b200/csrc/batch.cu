@@ -83,6 +83,8 @@ constexpr double LONG_STEPS = 4.0;
 // A search needs the blocks that cover its expected remaining work in this
 // many steps.
 constexpr double NEED_STEPS = 2.0;
+// shared memory of the search kernel: a staged bitmap of STAGED_BITMAP_BITS
+constexpr size_t STAGED_BYTES = (size_t)(1u << STAGED_BITMAP_BITS) / 8u;
 
 struct BatchDesc {
     FeWords wx, wy, wt;      // the search's stride for this step: L (2 half + 1) 8 G, affine
@@ -167,10 +169,15 @@ __global__ void __launch_bounds__(BLOCK) batch_init_kernel(const BatchArgs a) {
 // pool is exhausted. Every block of lanes belongs to one search, whose
 // descriptor gives its half, stride and bitmap. A block of a search whose
 // exact hits have reached its quota (counted by the previous steps' exact
-// kernels) is skipped: its lanes stay where they are.
+// kernels) is skipped: its lanes stay where they are. A prefix bitmap of up
+// to 16 bits is staged in shared memory, again only when the CTA's next
+// block belongs to another search (config 4 on B200: 19.52-19.55 s against
+// 19.67-19.82 s, the searches' small bitmaps no longer competing with the
+// table Q_m for L1).
 __global__ void __launch_bounds__(OG_LB_THREADS, OG_LB_MIN_BLOCKS) batch_search_kernel(const BatchArgs a) {
     const uint4* qtab = a.table;  // read through L1, as the single-search kernel does
-    __shared__ uint32_t item_s;
+    __shared__ uint32_t item_s, staged_s;  // staged_s: the search whose bitmap is in og_bitmap_s
+    if (threadIdx.x == 0) staged_s = NONE;
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) item_s = atomicAdd(&a.counters->work, 1u);
@@ -181,8 +188,18 @@ __global__ void __launch_bounds__(OG_LB_THREADS, OG_LB_MIN_BLOCKS) batch_search_
         if (sb.sidx == NONE) continue;
         const BatchDesc& d = a.descs[sb.sidx];
         if (d.quota && a.found[sb.sidx] >= d.quota) continue;
+        // the block's search decides this, the same for every thread; the
+        // barrier at the loop's top has retired every read of the old map
+        const bool staged = d.bitmap && d.bits <= STAGED_BITMAP_BITS;
+        if (staged && staged_s != sb.sidx) {
+            extern __shared__ uint32_t og_bitmap_s[];
+            const uint32_t words = (1u << d.bits) / 32u;
+            for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) og_bitmap_s[i] = d.bitmap[i];
+            __syncthreads();
+            if (threadIdx.x == 0) staged_s = sb.sidx;
+        }
         const uint32_t slot = item * BLOCK + threadIdx.x;
-        const Sink sink{d.bitmap, d.bits, a.surv, &a.counters->surv, a.surv_cap, sb.sidx, d.sbitmap, d.sbits};
+        const Sink sink{d.bitmap, d.bits, a.surv, &a.counters->surv, a.surv_cap, sb.sidx, d.sbitmap, d.sbits, staged};
         fe x = load_fe(a.lanes + 0 * a.slots + slot, a.slots);
         fe y = load_fe(a.lanes + 2 * a.slots + slot, a.slots);
         paired_rounds<false>(x, y, words_fe(d.wx), words_fe(d.wy), words_fe(d.wt), qtab, d.half, a.rounds,
@@ -547,7 +564,7 @@ int enqueue_step(og_batch* b, const BatchArgs& a, char* err, size_t errlen) {
     CU(cudaMemsetAsync(&a.counters->surv, 0, 3 * sizeof(uint32_t), b->stream));  // surv, hits, mismatch
     batch_init_kernel<<<b->nblocks, BLOCK, 0, b->stream>>>(a);
     CU(cudaGetLastError());
-    batch_search_kernel<<<b->grid, BLOCK, 0, b->stream>>>(a);
+    batch_search_kernel<<<b->grid, BLOCK, STAGED_BYTES, b->stream>>>(a);
     CU(cudaGetLastError());
     batch_exact_kernel<<<b->grid, 256, 0, b->stream>>>(a);
     CU(cudaGetLastError());
@@ -824,7 +841,7 @@ int og_batch_new(int ordinal, const og_batch_config* cfgp, og_batch** out, char*
     if (!b) return fail(err, errlen, OG_E_NOMEM, "host memory");
     b->device = ordinal;
     int per_sm = 0, sms = 0;
-    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_search_kernel, BLOCK, 0));
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_search_kernel, BLOCK, STAGED_BYTES));
     CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ordinal));
     const uint32_t fit = (uint32_t)std::max(1, per_sm);
     cfg.grid = cfg.grid == 0 ? fit : std::min(cfg.grid, fit);
@@ -1175,7 +1192,7 @@ int og_batch_tune(int ordinal, uint32_t searches, float max_step_ms, og_batch_co
     if (ordinal < 0 || ordinal >= count) return fail(err, errlen, OG_E_ARG, "device %d of %d", ordinal, count);
     CU(cudaSetDevice(ordinal));
     int per_sm = 0, sms = 0;
-    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_search_kernel, BLOCK, 0));
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_search_kernel, BLOCK, STAGED_BYTES));
     CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ordinal));
     const uint32_t fit = (uint32_t)std::max(1, per_sm);
     // a mix that never finishes: each search one ten-symbol prefix (50 bits)

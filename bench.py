@@ -358,8 +358,10 @@ def batched_leg(dev, shape, cap):
 
     t0 = time.perf_counter()
     b = B.Batch(dev, **shape, max_half=HALF)
+    t_created = time.perf_counter()
     for s in searches:
         b.admit(s.index, s.seed, s.prefixes, s.quota)
+    t_admitted = time.perf_counter()
     halves = {s.index: b.status(s.index).half for s in searches}
     steps = launches = 0
     dev_ms = 0.0
@@ -398,6 +400,7 @@ def batched_leg(dev, shape, cap):
         "batched": {"wall_s": batched_wall, "examined": examined, "keys_per_s": useful / batched_wall,
                     "examined_per_s": examined / batched_wall, "device_s": dev_ms / 1e3, "steps": steps,
                     "gpu_launches": launches, "halves": sorted(set(halves.values())),
+                    "create_s": t_created - t0, "admit_s": t_admitted - t_created,
                     "long_search_halves": [halves[i] for i in long_ids],
                     "shape": {**shape, "max_half": HALF, "inflight": 2}},
         "speedup_batched_over_plain": best_plain / batched_wall,

@@ -47,6 +47,9 @@ __global__ void __launch_bounds__(128) init_kernel(const InitArgs a) {
     }
 }
 
+// Staged: survivor records collected per warp in shared memory and written
+// 32 at a time (WarpStage), for indexes that let many candidates through.
+template <bool Staged>
 __global__ void __launch_bounds__(OG_LB_THREADS, OG_LB_MIN_BLOCKS) paired_kernel(const PairedArgs a) {
     // The table is read through L1, not staged in shared memory: every lane
     // of a warp loads the same entry, and leaving shared memory unused keeps
@@ -60,6 +63,8 @@ __global__ void __launch_bounds__(OG_LB_THREADS, OG_LB_MIN_BLOCKS) paired_kernel
     const uint32_t nblocks = a.lanes_n / blockDim.x;
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     const Sink sink{a.bitmap, a.bits, a.hits, a.counter, a.cap, a.search, a.sbitmap, a.sbits};
+    __shared__ uint4 stage_s[Staged ? (OG_LB_THREADS / 32) * STAGE_RECORDS * 3 : 1];
+    WarpStage st{stage_s + (Staged ? (threadIdx.x / 32) * STAGE_RECORDS * 3 : 0), 0};
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) item_s = atomicAdd(a.work, 1u);
@@ -70,7 +75,8 @@ __global__ void __launch_bounds__(OG_LB_THREADS, OG_LB_MIN_BLOCKS) paired_kernel
         fe x = load_fe(a.lanes + 0 * L + lane, L);
         fe y = load_fe(a.lanes + 2 * L + lane, L);
         paired_rounds<true>(x, y, words_fe(a.wx), words_fe(a.wy), words_fe(a.wt), qtab, a.half, a.rounds, a.scratch + slot, S,
-                      [&](const fe& v, uint32_t step) { test_emit(sink, v, lane, step); });
+                      [&](const fe& v, uint32_t step) { test_emit<Staged>(sink, v, lane, step, &st); });
+        if (Staged) stage_flush(sink, st);
         store_fe(a.lanes + 0 * L + lane, L, x);
         store_fe(a.lanes + 2 * L + lane, L, y);
     }
@@ -235,8 +241,10 @@ cudaError_t launch_paired(const PairedArgs& a, int block, int grid, cudaStream_t
         return cudaErrorInvalidValue;
     if (n == 2)
         paired_kernel2<<<grid, block, 0, s>>>(a);
+    else if (a.stage_records)
+        paired_kernel<true><<<grid, block, 0, s>>>(a);
     else
-        paired_kernel<<<grid, block, 0, s>>>(a);
+        paired_kernel<false><<<grid, block, 0, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -259,7 +267,7 @@ static cudaError_t info_of(const void* fn, int block, size_t smem, KernelInfo* i
 }
 
 cudaError_t paired_info(int block, uint32_t, uint32_t lanes_per_thread, KernelInfo* info) {
-    return info_of(lanes_per_thread == 2 ? (const void*)paired_kernel2 : (const void*)paired_kernel, block, 0, info);
+    return info_of(lanes_per_thread == 2 ? (const void*)paired_kernel2 : (const void*)paired_kernel<true>, block, 0, info);
 }
 
 // sized for a staged 16-bit bitmap, the most a chain launch takes

@@ -63,6 +63,7 @@ struct PairedArgs {
     uint32_t half;
     uint32_t rounds;         // rounds per launch
     uint32_t lanes_per_thread;  // 1 (paired_kernel) or 2 (paired_kernel2); S = CTAs x block x this
+    uint32_t stage_records;  // 1: survivors staged per warp in shared memory (one lane a thread only)
 };
 
 struct ChainArgs {

@@ -60,13 +60,48 @@ __device__ __forceinline__ uint32_t suffix_slot(const fe& y, uint32_t sbits) {
     return sbits >= 32 ? w : w & ((1u << sbits) - 1u);
 }
 
+// Survivor records staged per warp in shared memory, for dense indexes: a
+// warp collects up to STAGE_RECORDS records and writes them with one atomic
+// on the counter, where the direct append pays one for every warp-step that
+// carries a survivor (at config 3's 5 % survivors, four warp-steps in five).
+constexpr uint32_t STAGE_RECORDS = 32;
+
+struct WarpStage {
+    uint4* recs;  // this warp's STAGE_RECORDS records, three uint4 each, in shared memory
+    uint32_t n;   // records held; the same in every lane of the warp
+};
+
+// Writes a warp's staged records to the sink (all lanes of the warp call it
+// together). Records past the sink's room are counted, not written, as in
+// test_emit.
+__device__ __forceinline__ void stage_flush(const Sink& k, WarpStage& st) {
+    if (st.n == 0) return;
+    __syncwarp();
+    const unsigned me = threadIdx.x & 31u;
+    uint32_t base = 0;
+    if (me == 0) base = atomicAdd(k.counter, st.n);
+    base = __shfl_sync(FULL, base, 0);
+    if (me < st.n && base + me < k.cap) {
+        uint4* dst = reinterpret_cast<uint4*>(k.hits + base + me);
+        const uint4* src = st.recs + me * 3;
+        dst[0] = src[0];
+        dst[1] = src[1];
+        dst[2] = src[2];
+    }
+    __syncwarp();
+    st.n = 0;
+}
+
 // Canonicalises y, tests its slot in the prefix bitmap and in the suffix
 // bitmap (either lets it through; with neither, every candidate survives)
 // and appends a record for every lane of the warp that hit, with one atomic
-// per warp. Every lane of the warp must call this together (the kernels
-// keep warps converged: lane counts are whole blocks and loop trip counts
-// are uniform).
-__device__ __forceinline__ void test_emit(const Sink& k, const fe& yraw, uint32_t lane, uint32_t step) {
+// per warp; with `Staged`, into the warp's stage `st` instead (flushed when
+// full, and by the kernel at the end of each work item). Every lane of the
+// warp must call this together (the kernels keep warps converged: lane
+// counts are whole blocks and loop trip counts are uniform).
+template <bool Staged = false>
+__device__ __forceinline__ void test_emit(const Sink& k, const fe& yraw, uint32_t lane, uint32_t step,
+                                          WarpStage* st = nullptr) {
     // The canonical limbs the bitmaps read (0, 6 and 7), without the full
     // canonicalisation. Folding bit 255 adds 19 to limb 0; its carry reaches
     // limb 6 only through limbs 1..5 all ones, and the value can be p or
@@ -100,6 +135,20 @@ __device__ __forceinline__ void test_emit(const Sink& k, const fe& yraw, uint32_
     const unsigned mask = __ballot_sync(FULL, hit);
     if (mask == 0) return;
     const unsigned me = threadIdx.x & 31u;
+    if constexpr (Staged) {
+        const uint32_t count = (uint32_t)__popc(mask);
+        if (st->n + count > STAGE_RECORDS) stage_flush(k, *st);
+        if (hit) {
+            const uint32_t idx = st->n + (uint32_t)__popc(mask & ((1u << me) - 1u));
+            y = fe_canon(yraw);
+            uint4* rec = st->recs + idx * 3;
+            rec[0] = make_uint4(lane, step, k.search, 0u);
+            rec[1] = make_uint4(y.v[0], y.v[1], y.v[2], y.v[3]);
+            rec[2] = make_uint4(y.v[4], y.v[5], y.v[6], y.v[7]);
+        }
+        st->n += count;
+        return;
+    }
     const unsigned leader = __ffs(mask) - 1;
     uint32_t base = 0;
     if (me == leader) base = atomicAdd(k.counter, (uint32_t)__popc(mask));

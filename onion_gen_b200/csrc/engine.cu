@@ -18,6 +18,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/onion_gen_b200.h"
@@ -861,13 +862,51 @@ int og_engine_collect_matches(og_engine* e, og_match* out, size_t cap, size_t* n
     if (rc != OG_OK) return rc;
     const uint64_t L = e->cfg.lanes, slots = e->slots, R = e->cfg.rounds;
     const bool paired = e->cfg.scheme == OG_SCHEME_PAIRED;
+    // a record's offset, from its lane and step in this advance
+    const auto offset_of = [&](const HitRec& h) {
+        const uint64_t r = h.step / slots, i = h.step % slots;
+        const uint64_t w = (launch * R + r) * L + h.lane;
+        return paired ? 8 * (w * slots + 1 + i) : 8 * (w * slots + i);
+    };
+    static_assert(sizeof(og_match::packed) == sizeof(HitRec::y), "the packed key is the record's eight limbs");
+    static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "limbs copied as little-endian bytes");
+    if (!e->long_filters) {
+        // every record is a match: converted in place order, split over the
+        // host's threads when there are many (config 3 returns 4e7 an
+        // advance); the packed key is the limbs' little-endian bytes
+        if (matched > cap)
+            return fail(err, errlen, OG_E_CAPACITY, "%u matches and room for %zu in the caller's buffer", matched, cap);
+        const auto convert = [&](size_t lo, size_t hi) {
+            for (size_t j = lo; j < hi; j++) {
+                const HitRec& h = e->h_recs.p[j];
+                og_match& m = out[j];
+                m.offset = offset_of(h);
+                std::memcpy(m.packed, h.y, sizeof m.packed);
+                m.filter = h.pad;
+                m.pad = 0;
+            }
+        };
+        const size_t workers = matched >= (1u << 20) ? std::min<size_t>(16, std::max(1u, std::thread::hardware_concurrency())) : 1;
+        if (workers <= 1) {
+            convert(0, matched);
+        } else {
+            std::vector<std::thread> pool;
+            const size_t per = (matched + workers - 1) / workers;
+            for (size_t t = 0; t < workers; t++) {
+                const size_t lo = t * per, hi = std::min<size_t>(matched, lo + per);
+                if (lo < hi) pool.emplace_back(convert, lo, hi);
+            }
+            for (std::thread& th : pool) th.join();
+        }
+        *n = matched;
+        return OG_OK;
+    }
     size_t k = 0;
     for (uint32_t j = 0; j < matched; j++) {
         const HitRec& h = e->h_recs.p[j];
         og_match m;
         std::memset(&m, 0, sizeof m);
-        for (int q = 0; q < 8; q++)
-            for (int b = 0; b < 4; b++) m.packed[4 * q + b] = (uint8_t)(h.y[q] >> (8 * b));
+        std::memcpy(m.packed, h.y, sizeof m.packed);
         m.filter = h.pad;
         // With filters longer than the device tables reach, several can share
         // the 12 symbols the device compared: the host's match decides which
@@ -880,9 +919,7 @@ int og_engine_collect_matches(og_engine* e, og_match* out, size_t cap, size_t* n
         if (k == cap)
             return fail(err, errlen, OG_E_CAPACITY, "more than %zu matches and room for %zu in the caller's buffer",
                         cap, cap);
-        const uint64_t r = h.step / slots, i = h.step % slots;
-        const uint64_t w = (launch * R + r) * L + h.lane;
-        m.offset = paired ? 8 * (w * slots + 1 + i) : 8 * (w * slots + i);
+        m.offset = offset_of(h);
         out[k++] = m;
     }
     *n = k;

@@ -617,6 +617,24 @@ int enqueue_advance(og_engine* e, bool match, char* err, size_t errlen) {
 // Waits for the oldest flight and copies its records (survivors, or matches
 // for a matching flight) into h_recs on the copy stream, beside whatever
 // advance runs next. The flight is released whatever happens.
+// Runs body(lo, hi) over [0, n), split over up to 16 host threads when n is
+// large enough (2^20 records) for the threads to pay.
+template <class F>
+void over_threads(size_t n, F&& body) {
+    const size_t workers = n >= (1u << 20) ? std::min<size_t>(16, std::max(1u, std::thread::hardware_concurrency())) : 1;
+    if (workers <= 1) {
+        body((size_t)0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const size_t per = (n + workers - 1) / workers;
+    for (size_t t = 0; t < workers; t++) {
+        const size_t lo = t * per, hi = std::min(n, lo + per);
+        if (lo < hi) pool.emplace_back([&body, lo, hi] { body(lo, hi); });
+    }
+    for (std::thread& th : pool) th.join();
+}
+
 int collect_flight(og_engine* e, bool match, uint32_t* count, uint64_t* launch, char* err, size_t errlen) {
     if (e->inflight == 0) return fail(err, errlen, OG_E_STATE, "no advance in flight");
     og_engine::Flight& f = e->fl[e->head];
@@ -808,18 +826,17 @@ int og_engine_collect(og_engine* e, og_survivor* out, size_t cap, size_t* n, cha
     if (found > cap) return fail(err, errlen, OG_E_CAPACITY, "%u survivors and room for %zu in the caller's buffer", found, cap);
     const uint64_t L = e->cfg.lanes, slots = e->slots, R = e->cfg.rounds;
     const bool paired = e->cfg.scheme == OG_SCHEME_PAIRED;
-    for (uint32_t k = 0; k < found; k++) {
-        const HitRec& h = e->h_recs.p[k];
-        const uint64_t r = h.step / slots, i = h.step % slots;
-        const uint64_t w = (launch * R + r) * L + h.lane;
-        out[k].offset = paired ? 8 * (w * slots + 1 + i) : 8 * (w * slots + i);
-        for (int j = 0; j < 8; j++) {
-            out[k].packed[4 * j + 0] = (uint8_t)(h.y[j]);
-            out[k].packed[4 * j + 1] = (uint8_t)(h.y[j] >> 8);
-            out[k].packed[4 * j + 2] = (uint8_t)(h.y[j] >> 16);
-            out[k].packed[4 * j + 3] = (uint8_t)(h.y[j] >> 24);
+    static_assert(sizeof(og_survivor::packed) == sizeof(HitRec::y), "the packed key is the record's eight limbs");
+    static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "limbs copied as little-endian bytes");
+    over_threads(found, [&](size_t lo, size_t hi) {
+        for (size_t k = lo; k < hi; k++) {
+            const HitRec& h = e->h_recs.p[k];
+            const uint64_t r = h.step / slots, i = h.step % slots;
+            const uint64_t w = (launch * R + r) * L + h.lane;
+            out[k].offset = paired ? 8 * (w * slots + 1 + i) : 8 * (w * slots + i);
+            std::memcpy(out[k].packed, h.y, sizeof out[k].packed);
         }
-    }
+    });
     *n = found;
     return OG_OK;
 }
@@ -886,18 +903,7 @@ int og_engine_collect_matches(og_engine* e, og_match* out, size_t cap, size_t* n
                 m.pad = 0;
             }
         };
-        const size_t workers = matched >= (1u << 20) ? std::min<size_t>(16, std::max(1u, std::thread::hardware_concurrency())) : 1;
-        if (workers <= 1) {
-            convert(0, matched);
-        } else {
-            std::vector<std::thread> pool;
-            const size_t per = (matched + workers - 1) / workers;
-            for (size_t t = 0; t < workers; t++) {
-                const size_t lo = t * per, hi = std::min<size_t>(matched, lo + per);
-                if (lo < hi) pool.emplace_back(convert, lo, hi);
-            }
-            for (std::thread& th : pool) th.join();
-        }
+        over_threads(matched, convert);
         *n = matched;
         return OG_OK;
     }

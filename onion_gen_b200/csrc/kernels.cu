@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(OG_LB_THREADS, 5) chain_kernel(const ChainArgs
                 add_cached(X, Y, Z, T, words_fe(a.step_ypx), words_fe(a.step_ymx), words_fe(a.step_t2d));
             }
             if (L > 1) add_cached(X, Y, Z, T, words_fe(a.jump_ypx), words_fe(a.jump_ymx), words_fe(a.jump_t2d));
-            fe acc = fe_invert(run);
+            fe acc = block_invert(run);  // one inversion for the block's lanes
             const uint32_t base_step = r * a.n;
 #pragma unroll 1
             for (uint32_t t = a.n; t-- > 0;) {

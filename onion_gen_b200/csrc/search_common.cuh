@@ -9,6 +9,10 @@ namespace og {
 
 constexpr unsigned FULL = 0xffffffffu;
 
+#ifndef OG_LB_THREADS
+#define OG_LB_THREADS 128  // the most threads a block of the search kernels has
+#endif
+
 __device__ __forceinline__ fe load_fe(const uint4* p, size_t qstride) {
     const uint4 a = p[0];
     const uint4 b = p[qstride];
@@ -200,6 +204,71 @@ __device__ __forceinline__ uint32_t exact_owner(const MatchTables& t, const uint
     return 0xffffffffu;
 }
 
+__device__ __forceinline__ fe shfl_up_fe(const fe& v, unsigned d) {
+    fe r;
+#pragma unroll
+    for (int k = 0; k < 8; k++) r.v[k] = __shfl_up_sync(FULL, v.v[k], d);
+    return r;
+}
+
+__device__ __forceinline__ fe shfl_down_fe(const fe& v, unsigned d) {
+    fe r;
+#pragma unroll
+    for (int k = 0; k < 8; k++) r.v[k] = __shfl_down_sync(FULL, v.v[k], d);
+    return r;
+}
+
+__device__ __forceinline__ fe select_fe(bool c, const fe& a, const fe& b) {
+    fe r;
+#pragma unroll
+    for (int k = 0; k < 8; k++) r.v[k] = c ? a.v[k] : b.v[k];
+    return r;
+}
+
+// 1/v for every thread of the block with one field inversion for the whole
+// block: Montgomery's trick across its lanes. A warp executes an inversion
+// at the cost of all its lanes whether one lane or 32 need it, so one
+// inversion a block instead of one a warp saves three of every four on
+// 128-thread blocks. Within a warp, inclusive prefix and suffix products by
+// shuffles (five levels each, the missing neighbours taken as 1); across
+// warps, their totals in shared memory; thread 0 inverts the block's total;
+// then 1/v_i = (product before i) (product after i) / total. The inverse is
+// unique, so the result equals fe_invert's modulo p (0 when some v of the
+// block is 0, which the search's denominators never are). Every thread of
+// the block calls it together; blocks hold at most OG_LB_THREADS threads.
+// Not inlined, like fe_invert, so that the search loops' register
+// allocation does not change around it.
+static __device__ __noinline__ fe block_invert(const fe& v) {
+    __shared__ fe warp_total_s[OG_LB_THREADS / 32];
+    __shared__ fe inv_total_s;
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const fe one = fe_one();
+    fe pre = v, suf = v;
+#pragma unroll
+    for (unsigned d = 1; d < 32; d <<= 1) {
+        const fe lo = shfl_up_fe(pre, d), hi = shfl_down_fe(suf, d);
+        pre = fe_mulv(pre, select_fe(lane >= d, lo, one));
+        suf = fe_mulv(suf, select_fe(lane + d < 32, hi, one));
+    }
+    // exclusive: the products strictly before and after this lane
+    const fe before = select_fe(lane > 0, shfl_up_fe(pre, 1), one);
+    const fe after = select_fe(lane < 31, shfl_down_fe(suf, 1), one);
+    __syncthreads();  // earlier readers of the shared words are done
+    if (lane == 31) warp_total_s[warp] = pre;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        fe total = warp_total_s[0];
+        for (unsigned w = 1; w < nwarps; w++) total = fe_mulv(total, warp_total_s[w]);
+        inv_total_s = fe_invert(total);
+    }
+    // the other warps' totals, before and after this warp (the same in every lane)
+    fe others = one;
+    for (unsigned w = 0; w < nwarps; w++)
+        if (w != warp) others = fe_mulv(others, warp_total_s[w]);
+    __syncthreads();
+    return fe_mulv(fe_mulv(before, after), fe_mulv(others, inv_total_s));
+}
+
 // p3 + cached addend with Z = 1: seven multiplications
 // (the formulas of src/curve.rs:130-175 with the addend's Z scaled away).
 __device__ __forceinline__ void add_cached(fe& X, fe& Y, fe& Z, fe& T, const fe& ypx, const fe& ymx,
@@ -225,9 +294,6 @@ __device__ __forceinline__ void add_cached(fe& X, fe& Y, fe& Z, fe& T, const fe&
 // (Park = false): the 12 KB of shared memory a block takes it from L1,
 // and that kernel, whose CTAs move between searches and their bitmaps,
 // ran 10 % slower parked.
-#ifndef OG_LB_THREADS
-#define OG_LB_THREADS 128  // the most threads a block of the search kernels has
-#endif
 constexpr int PARK_STRIDE = OG_LB_THREADS;
 
 __device__ __forceinline__ void park_fe(uint4* park, int k, const fe& v) {
@@ -293,7 +359,10 @@ __device__ __forceinline__ void paired_rounds(fe& x, fe& y, const fe& wx, const 
             store_fe(SCR(2 * m + 1, 1), L, d1);
             run = fe_mulv(run, d1);
         }
-        fe acc = fe_invert(run);
+        // one inversion for the block's lanes where the centre is parked; the
+        // batched kernel keeps it in registers, which the call would save and
+        // restore (measured 1 % slower there), so it inverts per lane
+        fe acc = Park ? block_invert(run) : fe_invert(run);
         const uint32_t base_step = r * slots;
         visit(centre(1), base_step + half);
 #pragma unroll 1

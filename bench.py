@@ -413,10 +413,12 @@ def batched_leg(dev, shape, cap, kernel_rate):
             "share_of_work": useful_long / useful,
             "plain_wall_s": best_arm["long_searches_wall_s"],
             "kernel_rate": kernel_rate,
-            "bound_note": "a batch examines the long searches' candidates no faster than the single-search kernel "
-            "at half 2048 (kernel_rate, the plain line's keys/s), so even with the short searches free the speedup "
-            "over the faster plain arm is at most its wall / (those candidates / kernel_rate)",
-            "speedup_bound": best_plain / (useful_long / kernel_rate) if kernel_rate else None,
+            "bound_note": "no engine examines candidates faster than the single-search kernel at half 2048 "
+            "(kernel_rate, the plain line's keys/s): over the faster plain arm a batch is at most its wall / "
+            "(all candidates to quota / kernel_rate) faster, and at most its wall / (the long searches' "
+            "candidates / kernel_rate) even with the short searches free",
+            "speedup_bound": best_plain / (useful / kernel_rate) if kernel_rate else None,
+            "speedup_bound_short_free": best_plain / (useful_long / kernel_rate) if kernel_rate else None,
         },
         "unit": "keys/s (candidates up to each search's quota-th hit, wall clock)",
     }
@@ -563,10 +565,23 @@ def config3_leg(dev, peak, steps=2):
     }
 
 
+BLOCK_LANES = 128  # lanes a block of the search kernels, which share one inversion
+
+
+def block_inversion_pp():
+    """Partial products a lane spends on its share of the block's one
+    inversion: 16 multiplications of its own (two five-step warp scans, the
+    other three warps' totals, the last three products) and 1/128 of thread
+    0's (three multiplications for the block's product and the inversion,
+    254 squarings of 36 products and 11 multiplications)."""
+    return 16 * 64 + (14 * 64 + 254 * 36) / BLOCK_LANES
+
+
 def pp_per_candidate(half):
-    """Partial products per candidate of the paired round: (21 + 10 half)
-    multiplications of 64 and 254 squarings of 36, over 2 half + 1 keys."""
-    return ((21 + 10 * half) * 64 + 254 * 36) / (2 * half + 1)
+    """Partial products per candidate of the paired round: 10 + 10 half
+    multiplications of 64 and the lane's share of the block's inversion,
+    over 2 half + 1 keys."""
+    return ((10 + 10 * half) * 64 + block_inversion_pp()) / (2 * half + 1)
 
 
 def small_case(args):
@@ -659,9 +674,9 @@ def config3_small_case(args):
 def chain_pp_per_candidate(n):
     """Partial products per candidate of the chain scheme (the config-1
     contract, src/batch.rs:78-122): 7 multiplications for the +8G step, 4 for
-    Montgomery's trick and y / Z, and one inversion (254 squarings of 36
-    products, 11 multiplications) per n steps."""
-    return (11 * 64 * n + 11 * 64 + 254 * 36) / n
+    Montgomery's trick and y / Z, and the lane's share of the block's
+    inversion per n steps."""
+    return (11 * 64 * n + block_inversion_pp()) / n
 
 
 def chain_leg(dev, peak):

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -168,6 +169,8 @@ struct og_engine {
     uint32_t head = 0, inflight = 0;
     cudaStream_t cstream = nullptr;  // record copies, beside the next advance's kernels
     HostBuf<HitRec> h_recs;
+    static constexpr int COPY_CHUNKS = 16;
+    cudaEvent_t chunk_ev[COPY_CHUNKS] = {};  // a chunk of the records has reached h_recs
     PairedArgs pa{};
     ChainArgs ca{};
     uint64_t bitmap_hash = 0;  // of the bitmap the engine was created with
@@ -199,6 +202,8 @@ struct og_engine {
             if (f.ev1) cudaEventDestroy(f.ev1);
             if (f.done) cudaEventDestroy(f.done);
         }
+        for (cudaEvent_t ev : chunk_ev)
+            if (ev) cudaEventDestroy(ev);
     }
 };
 
@@ -353,6 +358,7 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
         CU(cudaEventCreate(&f.ev1));
         CU(cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming));
     }
+    for (cudaEvent_t& ev : e->chunk_ev) CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
 
     const size_t L = cfg.lanes;
     const uint64_t batch = (uint64_t)L * slots * cfg.rounds;
@@ -614,28 +620,17 @@ int enqueue_advance(og_engine* e, bool match, char* err, size_t errlen) {
     return OG_OK;
 }
 
-// Waits for the oldest flight and copies its records (survivors, or matches
-// for a matching flight) into h_recs on the copy stream, beside whatever
-// advance runs next. The flight is released whatever happens.
-// Runs body(lo, hi) over [0, n), split over up to 16 host threads when n is
-// large enough (2^20 records) for the threads to pay.
-template <class F>
-void over_threads(size_t n, F&& body) {
-    const size_t workers = n >= (1u << 20) ? std::min<size_t>(16, std::max(1u, std::thread::hardware_concurrency())) : 1;
-    if (workers <= 1) {
-        body((size_t)0, n);
-        return;
-    }
-    std::vector<std::thread> pool;
-    const size_t per = (n + workers - 1) / workers;
-    for (size_t t = 0; t < workers; t++) {
-        const size_t lo = t * per, hi = std::min(n, lo + per);
-        if (lo < hi) pool.emplace_back([&body, lo, hi] { body(lo, hi); });
-    }
-    for (std::thread& th : pool) th.join();
+// Host threads that convert n records: up to 16 when n is large enough
+// (2^20 records) for the threads to pay.
+size_t host_workers(size_t n) {
+    return n >= (1u << 20) ? std::min<size_t>(16, std::max(1u, std::thread::hardware_concurrency())) : 1;
 }
 
-int collect_flight(og_engine* e, bool match, uint32_t* count, uint64_t* launch, char* err, size_t errlen) {
+// Waits for the oldest flight and checks its counts. The flight is released
+// whatever happens; its records (survivors, or matches for a matching
+// flight) are left on the device for copy_records, at *src.
+int collect_flight(og_engine* e, bool match, uint32_t* count, uint64_t* launch, const HitRec** src, char* err,
+                   size_t errlen) {
     if (e->inflight == 0) return fail(err, errlen, OG_E_STATE, "no advance in flight");
     og_engine::Flight& f = e->fl[e->head];
     if (f.match != match)
@@ -659,13 +654,58 @@ int collect_flight(og_engine* e, bool match, uint32_t* count, uint64_t* launch, 
         return fail(err, errlen, OG_E_VERIFY,
                     "%u survivors' keys recomputed from their offsets differ from the search kernel's",
                     f.h_counts.p[2]);
-    const uint32_t n = match ? f.h_counts.p[1] : found;  // matches are at most the survivors
-    if (n) {
-        CU(cudaMemcpyAsync(e->h_recs.p, match ? f.matches.p : f.hits.p, (size_t)n * sizeof(HitRec),
-                           cudaMemcpyDeviceToHost, e->cstream));
-        CU(cudaStreamSynchronize(e->cstream));
+    *count = match ? f.h_counts.p[1] : found;  // matches are at most the survivors
+    *src = match ? f.matches.p : f.hits.p;
+    return OG_OK;
+}
+
+// Copies n records from the device into h_recs on the copy stream, in up to
+// COPY_CHUNKS chunks of at least 2^18 records, and runs body(lo, hi) over
+// every record as soon as its chunk has arrived: the host threads convert
+// one chunk while the next ones cross PCIe (config 3 returns 4e7 matches,
+// 1.9 GB, an advance). Each of the host_workers(n) threads takes its slice
+// of every chunk. On an error every copy issued has ended before it returns.
+template <class F>
+int copy_records(og_engine* e, const HitRec* src, size_t n, F&& body, char* err, size_t errlen) {
+    if (n == 0) return OG_OK;
+    constexpr size_t MIN_CHUNK = 1u << 18;
+    const size_t chunks = std::min<size_t>(og_engine::COPY_CHUNKS, (n + MIN_CHUNK - 1) / MIN_CHUNK);
+    const size_t per = (n + chunks - 1) / chunks;
+    cudaError_t ce = cudaSuccess;
+    for (size_t c = 0; c < chunks && ce == cudaSuccess; c++) {
+        const size_t lo = c * per, hi = std::min(n, lo + per);
+        ce = cudaMemcpyAsync(e->h_recs.p + lo, src + lo, (hi - lo) * sizeof(HitRec), cudaMemcpyDeviceToHost,
+                             e->cstream);
+        if (ce == cudaSuccess) ce = cudaEventRecord(e->chunk_ev[c], e->cstream);
     }
-    *count = n;
+    std::atomic<int> failed{(int)ce};
+    const auto work = [&](size_t t, size_t workers) {
+        for (size_t c = 0; c < chunks && failed.load() == cudaSuccess; c++) {
+            const cudaError_t we = cudaEventSynchronize(e->chunk_ev[c]);
+            if (we != cudaSuccess) {
+                failed.store((int)we);
+                return;
+            }
+            const size_t lo = c * per, hi = std::min(n, lo + per), slice = (hi - lo + workers - 1) / workers;
+            const size_t a = std::min(hi, lo + t * slice), b = std::min(hi, a + slice);
+            if (a < b) body(a, b);
+        }
+    };
+    const size_t workers = host_workers(n);
+    if (ce == cudaSuccess) {
+        if (workers <= 1) {
+            work(0, 1);
+        } else {
+            std::vector<std::thread> pool;
+            for (size_t t = 0; t < workers; t++) pool.emplace_back([&work, t, workers] { work(t, workers); });
+            for (std::thread& th : pool) th.join();
+        }
+    }
+    if (failed.load() != cudaSuccess) {
+        cudaStreamSynchronize(e->cstream);
+        return fail(err, errlen, OG_E_DEVICE, "copying %zu records back: %s", n,
+                    cuda_text((cudaError_t)failed.load()).c_str());
+    }
     return OG_OK;
 }
 }  // namespace
@@ -821,14 +861,15 @@ int og_engine_collect(og_engine* e, og_survivor* out, size_t cap, size_t* n, cha
     *n = 0;
     uint32_t found = 0;
     uint64_t launch = 0;
-    int rc = collect_flight(e, false, &found, &launch, err, errlen);
+    const HitRec* src = nullptr;
+    int rc = collect_flight(e, false, &found, &launch, &src, err, errlen);
     if (rc != OG_OK) return rc;
     if (found > cap) return fail(err, errlen, OG_E_CAPACITY, "%u survivors and room for %zu in the caller's buffer", found, cap);
     const uint64_t L = e->cfg.lanes, slots = e->slots, R = e->cfg.rounds;
     const bool paired = e->cfg.scheme == OG_SCHEME_PAIRED;
     static_assert(sizeof(og_survivor::packed) == sizeof(HitRec::y), "the packed key is the record's eight limbs");
     static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "limbs copied as little-endian bytes");
-    over_threads(found, [&](size_t lo, size_t hi) {
+    rc = copy_records(e, src, found, [&](size_t lo, size_t hi) {
         for (size_t k = lo; k < hi; k++) {
             const HitRec& h = e->h_recs.p[k];
             const uint64_t r = h.step / slots, i = h.step % slots;
@@ -836,7 +877,8 @@ int og_engine_collect(og_engine* e, og_survivor* out, size_t cap, size_t* n, cha
             out[k].offset = paired ? 8 * (w * slots + 1 + i) : 8 * (w * slots + i);
             std::memcpy(out[k].packed, h.y, sizeof out[k].packed);
         }
-    });
+    }, err, errlen);
+    if (rc != OG_OK) return rc;
     *n = found;
     return OG_OK;
 }
@@ -875,7 +917,8 @@ int og_engine_collect_matches(og_engine* e, og_match* out, size_t cap, size_t* n
     *n = 0;
     uint32_t matched = 0;
     uint64_t launch = 0;
-    int rc = collect_flight(e, true, &matched, &launch, err, errlen);
+    const HitRec* src = nullptr;
+    int rc = collect_flight(e, true, &matched, &launch, &src, err, errlen);
     if (rc != OG_OK) return rc;
     const uint64_t L = e->cfg.lanes, slots = e->slots, R = e->cfg.rounds;
     const bool paired = e->cfg.scheme == OG_SCHEME_PAIRED;
@@ -888,12 +931,11 @@ int og_engine_collect_matches(og_engine* e, og_match* out, size_t cap, size_t* n
     static_assert(sizeof(og_match::packed) == sizeof(HitRec::y), "the packed key is the record's eight limbs");
     static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "limbs copied as little-endian bytes");
     if (!e->long_filters) {
-        // every record is a match: converted in place order, split over the
-        // host's threads when there are many (config 3 returns 4e7 an
-        // advance); the packed key is the limbs' little-endian bytes
+        // every record is a match: converted in place order as its chunk
+        // arrives; the packed key is the limbs' little-endian bytes
         if (matched > cap)
             return fail(err, errlen, OG_E_CAPACITY, "%u matches and room for %zu in the caller's buffer", matched, cap);
-        const auto convert = [&](size_t lo, size_t hi) {
+        rc = copy_records(e, src, matched, [&](size_t lo, size_t hi) {
             for (size_t j = lo; j < hi; j++) {
                 const HitRec& h = e->h_recs.p[j];
                 og_match& m = out[j];
@@ -902,11 +944,13 @@ int og_engine_collect_matches(og_engine* e, og_match* out, size_t cap, size_t* n
                 m.filter = h.pad;
                 m.pad = 0;
             }
-        };
-        over_threads(matched, convert);
+        }, err, errlen);
+        if (rc != OG_OK) return rc;
         *n = matched;
         return OG_OK;
     }
+    rc = copy_records(e, src, matched, [](size_t, size_t) {}, err, errlen);
+    if (rc != OG_OK) return rc;
     size_t k = 0;
     for (uint32_t j = 0; j < matched; j++) {
         const HitRec& h = e->h_recs.p[j];

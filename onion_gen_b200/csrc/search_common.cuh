@@ -291,9 +291,8 @@ __device__ __forceinline__ void add_cached(fe& X, fe& Y, fe& Z, fe& T, const fe&
 // registers for the whole loop. The 24 registers this frees took the
 // single-search kernel at 96 registers from 72 bytes of spills to 4 and
 // from 20.6 to 20.8 G keys/s on B200. The batched kernel does not park
-// (Park = false): the 12 KB of shared memory a block takes it from L1,
-// and that kernel, whose CTAs move between searches and their bitmaps,
-// ran 10 % slower parked.
+// (Park = false): with its staged bitmap the 12 KB a block would leave L1
+// too small for the table Q_m at half 2048, and it ran 6 % slower parked.
 constexpr int PARK_STRIDE = OG_LB_THREADS;
 
 __device__ __forceinline__ void park_fe(uint4* park, int k, const fe& v) {

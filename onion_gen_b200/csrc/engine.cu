@@ -375,8 +375,10 @@ int build_engine(int ordinal, const uint8_t start[128], og_engine_config cfg, co
         if (rc) return rc;
         e->grid = std::max<uint32_t>(1, resident / (cfg.block * lpt));
         if (cfg.scheme == OG_SCHEME_CHAIN) e->grid = std::min<uint32_t>(e->grid, (uint32_t)(L / cfg.block));
-        // one scratch column per lane a thread holds
-        CU(e->scratch.alloc((size_t)e->grid * cfg.block * lpt * elems * 4));
+        // one scratch column per lane a thread holds; a chain CTA's rows hold
+        // CHAIN_ROW threads whatever its block
+        const size_t row = cfg.scheme == OG_SCHEME_CHAIN ? CHAIN_ROW : (size_t)cfg.block * lpt;
+        CU(e->scratch.alloc((size_t)e->grid * row * elems * 4));
     }
     for (og_engine::Flight& f : e->fl) {
         CU(f.counts.alloc(4));

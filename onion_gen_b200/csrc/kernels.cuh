@@ -66,11 +66,16 @@ struct PairedArgs {
     uint32_t stage_records;  // 1: survivors staged per warp in shared memory (one lane a thread only)
 };
 
+// Rows of a chain CTA's scratch hold this many threads (the largest block).
+constexpr uint32_t CHAIN_ROW = 128;
+
 struct ChainArgs {
     uint4* lanes;            // projective points: ({X,Y,Z,T} * 2 + q) * L + lane
-    uint4* scratch;          // ((t * 2 + {num,den}) * 2 + q) * S + slot, t < n (per persistent CTA slot)
+    // per persistent CTA c a region of CHAIN_ROW * 4 n uint4 from c CHAIN_ROW 4 n:
+    // thread j's step t, part w ({num,den}), half q at ((t * 2 + w) * 2 + q) CHAIN_ROW + j
+    uint4* scratch;
     uint32_t* work;          // blocks of lanes taken so far this launch (starts at 0)
-    uint32_t slots_n;        // S = persistent CTAs x block
+    uint32_t slots_n;        // persistent CTAs x block
     const uint32_t* bitmap;
     uint32_t bits;
     HitRec* hits;

@@ -513,17 +513,17 @@ def config3_leg(dev, peak, steps=2):
     batch = eng.batch()
     advances = -(-CANDIDATES_PER_STEP // batch)
     eng.advance_matches_raw()  # warm-up
-    # the matches land in the engine's own og_match buffer through the C
-    # ABI, as a caller in C takes them; only the sampled ones become Python
-    # objects
+    # the matches cross into the engine's pinned host memory, in og_match's
+    # layout, and og_engine_collect_matches_view hands them over there, as a
+    # caller in C takes them; only the sampled ones become Python objects
     import ctypes as C
 
-    buf, room = eng._mbuf, eng.room()
     kernel_ms = 0.0
     matches = checked = 0
     rng = np.random.default_rng(3)
     err = N.errbuf()
     nout = C.c_size_t()
+    view = C.c_void_p()
     t0 = time.perf_counter()
     total = steps * advances
     launched = 0
@@ -531,10 +531,11 @@ def config3_leg(dev, peak, steps=2):
         while launched - i < 2 and launched < total:
             N.check(N.lib.og_engine_launch_matches(eng._h, err, 512), err)
             launched += 1
-        N.check(N.lib.og_engine_collect_matches(eng._h, buf, room, C.byref(nout), err, 512), err)
+        N.check(N.lib.og_engine_collect_matches_view(eng._h, C.byref(view), C.byref(nout), err, 512), err)
         kernel_ms += eng.last_kernel_ms()
         m = nout.value
         matches += m
+        buf = (N.Match * m).from_address(view.value) if m else []
         for j in rng.choice(m, size=min(64, m), replace=False):
             h = buf[int(j)]
             pk, _ = key.check_hit(seed, int(h.offset), bytes(h.packed))
@@ -559,8 +560,9 @@ def config3_leg(dev, peak, steps=2):
         "matches": matches,
         "match_fraction": matches / n,
         "matches_rederived": checked,
-        "e2e_note": "every match crosses to the host into the og_match buffer (48 bytes each, 5 % of the "
-        "candidates), with 64 of each advance's matches re-derived and confirmed on the host",
+        "e2e_note": "every match crosses to the host in og_match's layout (48 bytes each, 5 % of the "
+        "candidates) into the engine's pinned memory, handed over there by og_engine_collect_matches_view, "
+        "with 64 of each advance's matches re-derived and confirmed on the host",
         "unit": "keys/s (CUDA events on the search kernel; e2e: wall clock with every match copied back)",
     }
 

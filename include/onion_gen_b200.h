@@ -185,6 +185,14 @@ int og_engine_advance_matches(og_engine* e, og_match* out, size_t cap, size_t* n
  * og_engine_collect. */
 int og_engine_launch_matches(og_engine* e, char* err, size_t errlen);
 int og_engine_collect_matches(og_engine* e, og_match* out, size_t cap, size_t* n, char* err, size_t errlen);
+/* og_engine_collect_matches without the copy into the caller's buffer: the
+ * oldest advance's `*n` matches are left in the engine's own pinned host
+ * memory, which the device writes into directly, and `*matches` points at
+ * them. They stay valid until the next collect of any kind or
+ * og_engine_free; a caller that keeps them copies them first. The same
+ * errors as og_engine_collect_matches, bar OG_E_CAPACITY (the engine's room
+ * holds every match). */
+int og_engine_collect_matches_view(og_engine* e, const og_match** matches, size_t* n, char* err, size_t errlen);
 
 void og_engine_free(og_engine* e);
 

@@ -159,6 +159,7 @@ def _load():
     sig("og_engine_collect", I, [P, P, SZ, C.POINTER(SZ), B, SZ])
     sig("og_engine_launch_matches", I, [P, B, SZ])
     sig("og_engine_collect_matches", I, [P, P, SZ, C.POINTER(SZ), B, SZ])
+    sig("og_engine_collect_matches_view", I, [P, C.POINTER(P), C.POINTER(SZ), B, SZ])
     sig("og_engine_last_kernel_ms", C.c_float, [P])
     sig("og_engine_match_on_device", I, [P, P, B, SZ])
     sig("og_engine_new_filters", I, [I, B, P, P, C.POINTER(P), B, SZ])

@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -160,7 +161,8 @@ struct og_engine {
     // are shared, the launches being ordered on one stream.
     struct Flight {
         DevBuf<uint32_t> counts;  // survivors, matches, mismatched suffix keys
-        DevBuf<HitRec> hits, matches;
+        DevBuf<HitRec> hits;
+        DevBuf<MatchRec> matches;
         HostBuf<uint32_t> h_counts;
         cudaEvent_t ev0 = nullptr, ev1 = nullptr, done = nullptr;
         uint64_t launch = 0;
@@ -168,7 +170,7 @@ struct og_engine {
     } fl[2];
     uint32_t head = 0, inflight = 0;
     cudaStream_t cstream = nullptr;  // record copies, beside the next advance's kernels
-    HostBuf<HitRec> h_recs;
+    HostBuf<HitRec> h_recs;  // pinned: survivors, or (as MatchRec, the same size) matches
     static constexpr int COPY_CHUNKS = 16;
     cudaEvent_t chunk_ev[COPY_CHUNKS] = {};  // a chunk of the records has reached h_recs
     PairedArgs pa{};
@@ -629,9 +631,9 @@ size_t host_workers(size_t n) {
 }
 
 // Waits for the oldest flight and checks its counts. The flight is released
-// whatever happens; its records (survivors, or matches for a matching
-// flight) are left on the device for copy_records, at *src.
-int collect_flight(og_engine* e, bool match, uint32_t* count, uint64_t* launch, const HitRec** src, char* err,
+// whatever happens; its records (HitRec survivors, or MatchRec matches for a
+// matching flight) are left on the device for copy_records, at *src.
+int collect_flight(og_engine* e, bool match, uint32_t* count, uint64_t* launch, const void** src, char* err,
                    size_t errlen) {
     if (e->inflight == 0) return fail(err, errlen, OG_E_STATE, "no advance in flight");
     og_engine::Flight& f = e->fl[e->head];
@@ -657,27 +659,29 @@ int collect_flight(og_engine* e, bool match, uint32_t* count, uint64_t* launch, 
                     "%u survivors' keys recomputed from their offsets differ from the search kernel's",
                     f.h_counts.p[2]);
     *count = match ? f.h_counts.p[1] : found;  // matches are at most the survivors
-    *src = match ? f.matches.p : f.hits.p;
+    *src = match ? (const void*)f.matches.p : (const void*)f.hits.p;
     return OG_OK;
 }
 
-// Copies n records from the device into h_recs on the copy stream, in up to
-// COPY_CHUNKS chunks of at least 2^18 records, and runs body(lo, hi) over
-// every record as soon as its chunk has arrived: the host threads convert
-// one chunk while the next ones cross PCIe (config 3 returns 4e7 matches,
-// 1.9 GB, an advance). Each of the host_workers(n) threads takes its slice
-// of every chunk. On an error every copy issued has ended before it returns.
-template <class F>
-int copy_records(og_engine* e, const HitRec* src, size_t n, F&& body, char* err, size_t errlen) {
+// Copies n records of type Rec (HitRec or MatchRec, 48 bytes) from the
+// device into h_recs on the copy stream, in up to COPY_CHUNKS chunks of at
+// least 2^18 records, and runs body(lo, hi) over every record as soon as its
+// chunk has arrived: the host threads convert one chunk while the next ones
+// cross PCIe (config 3 returns 4e7 matches, 1.9 GB, an advance). Each of
+// `workers` threads (host_workers(n) by default) takes its slice of every
+// chunk. On an error every copy issued has ended before it returns.
+template <class Rec, class F>
+int copy_records(og_engine* e, const Rec* src, size_t n, F&& body, char* err, size_t errlen, size_t workers = 0) {
+    static_assert(sizeof(Rec) == sizeof(HitRec), "the staging holds either record");
     if (n == 0) return OG_OK;
+    Rec* const stage = reinterpret_cast<Rec*>(e->h_recs.p);
     constexpr size_t MIN_CHUNK = 1u << 18;
     const size_t chunks = std::min<size_t>(og_engine::COPY_CHUNKS, (n + MIN_CHUNK - 1) / MIN_CHUNK);
     const size_t per = (n + chunks - 1) / chunks;
     cudaError_t ce = cudaSuccess;
     for (size_t c = 0; c < chunks && ce == cudaSuccess; c++) {
         const size_t lo = c * per, hi = std::min(n, lo + per);
-        ce = cudaMemcpyAsync(e->h_recs.p + lo, src + lo, (hi - lo) * sizeof(HitRec), cudaMemcpyDeviceToHost,
-                             e->cstream);
+        ce = cudaMemcpyAsync(stage + lo, src + lo, (hi - lo) * sizeof(Rec), cudaMemcpyDeviceToHost, e->cstream);
         if (ce == cudaSuccess) ce = cudaEventRecord(e->chunk_ev[c], e->cstream);
     }
     std::atomic<int> failed{(int)ce};
@@ -693,7 +697,7 @@ int copy_records(og_engine* e, const HitRec* src, size_t n, F&& body, char* err,
             if (a < b) body(a, b);
         }
     };
-    const size_t workers = host_workers(n);
+    if (workers == 0) workers = host_workers(n);
     if (ce == cudaSuccess) {
         if (workers <= 1) {
             work(0, 1);
@@ -710,6 +714,31 @@ int copy_records(og_engine* e, const HitRec* src, size_t n, F&& body, char* err,
     }
     return OG_OK;
 }
+// With filters longer than the device tables reach, several can share the
+// 12 symbols the device compared: the host's match (FilterSet::match_key)
+// decides which, if any, each prefix record matches. Keeps the confirmed
+// records, in order, at the front of `recs` and returns their count.
+size_t confirm_matches(og_engine* e, MatchRec* recs, size_t n) {
+    static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "limbs read as little-endian bytes");
+    size_t k = 0;
+    for (size_t j = 0; j < n; j++) {
+        MatchRec m = recs[j];
+        if (m.filter < e->prefix_count) {
+            const long f = e->fs.match_key(reinterpret_cast<const uint8_t*>(m.y));
+            if (f < 0) continue;
+            m.filter = (uint32_t)f;
+        }
+        recs[k++] = m;
+    }
+    return k;
+}
+
+// The device writes matches in the caller's layout.
+static_assert(sizeof(og_match) == sizeof(MatchRec) && offsetof(og_match, offset) == offsetof(MatchRec, offset) &&
+                  offsetof(og_match, packed) == offsetof(MatchRec, y) &&
+                  offsetof(og_match, filter) == offsetof(MatchRec, filter) &&
+                  offsetof(og_match, pad) == offsetof(MatchRec, pad),
+              "MatchRec is og_match's layout");
 }  // namespace
 
 extern "C" {
@@ -863,7 +892,7 @@ int og_engine_collect(og_engine* e, og_survivor* out, size_t cap, size_t* n, cha
     *n = 0;
     uint32_t found = 0;
     uint64_t launch = 0;
-    const HitRec* src = nullptr;
+    const void* src = nullptr;
     int rc = collect_flight(e, false, &found, &launch, &src, err, errlen);
     if (rc != OG_OK) return rc;
     if (found > cap) return fail(err, errlen, OG_E_CAPACITY, "%u survivors and room for %zu in the caller's buffer", found, cap);
@@ -871,7 +900,7 @@ int og_engine_collect(og_engine* e, og_survivor* out, size_t cap, size_t* n, cha
     const bool paired = e->cfg.scheme == OG_SCHEME_PAIRED;
     static_assert(sizeof(og_survivor::packed) == sizeof(HitRec::y), "the packed key is the record's eight limbs");
     static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "limbs copied as little-endian bytes");
-    rc = copy_records(e, src, found, [&](size_t lo, size_t hi) {
+    rc = copy_records(e, static_cast<const HitRec*>(src), found, [&](size_t lo, size_t hi) {
         for (size_t k = lo; k < hi; k++) {
             const HitRec& h = e->h_recs.p[k];
             const uint64_t r = h.step / slots, i = h.step % slots;
@@ -919,62 +948,47 @@ int og_engine_collect_matches(og_engine* e, og_match* out, size_t cap, size_t* n
     *n = 0;
     uint32_t matched = 0;
     uint64_t launch = 0;
-    const HitRec* src = nullptr;
+    const void* src = nullptr;
     int rc = collect_flight(e, true, &matched, &launch, &src, err, errlen);
     if (rc != OG_OK) return rc;
-    const uint64_t L = e->cfg.lanes, slots = e->slots, R = e->cfg.rounds;
-    const bool paired = e->cfg.scheme == OG_SCHEME_PAIRED;
-    // a record's offset, from its lane and step in this advance
-    const auto offset_of = [&](const HitRec& h) {
-        const uint64_t r = h.step / slots, i = h.step % slots;
-        const uint64_t w = (launch * R + r) * L + h.lane;
-        return paired ? 8 * (w * slots + 1 + i) : 8 * (w * slots + i);
-    };
-    static_assert(sizeof(og_match::packed) == sizeof(HitRec::y), "the packed key is the record's eight limbs");
-    static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "limbs copied as little-endian bytes");
+    const MatchRec* dev = static_cast<const MatchRec*>(src);
+    const MatchRec* stage = reinterpret_cast<const MatchRec*>(e->h_recs.p);
     if (!e->long_filters) {
-        // every record is a match: converted in place order as its chunk
-        // arrives; the packed key is the limbs' little-endian bytes
+        // every record is a match, already in the caller's layout: each
+        // chunk is copied out as soon as it arrives
         if (matched > cap)
             return fail(err, errlen, OG_E_CAPACITY, "%u matches and room for %zu in the caller's buffer", matched, cap);
-        rc = copy_records(e, src, matched, [&](size_t lo, size_t hi) {
-            for (size_t j = lo; j < hi; j++) {
-                const HitRec& h = e->h_recs.p[j];
-                og_match& m = out[j];
-                m.offset = offset_of(h);
-                std::memcpy(m.packed, h.y, sizeof m.packed);
-                m.filter = h.pad;
-                m.pad = 0;
-            }
+        rc = copy_records(e, dev, matched, [&](size_t lo, size_t hi) {
+            std::memcpy(out + lo, stage + lo, (hi - lo) * sizeof(og_match));
         }, err, errlen);
         if (rc != OG_OK) return rc;
         *n = matched;
         return OG_OK;
     }
-    rc = copy_records(e, src, matched, [](size_t, size_t) {}, err, errlen);
+    rc = copy_records(e, dev, matched, [](size_t, size_t) {}, err, errlen, 1);
     if (rc != OG_OK) return rc;
-    size_t k = 0;
-    for (uint32_t j = 0; j < matched; j++) {
-        const HitRec& h = e->h_recs.p[j];
-        og_match m;
-        std::memset(&m, 0, sizeof m);
-        std::memcpy(m.packed, h.y, sizeof m.packed);
-        m.filter = h.pad;
-        // With filters longer than the device tables reach, several can share
-        // the 12 symbols the device compared: the host's match decides which
-        // (if any) matches.
-        if (e->long_filters && h.pad < e->prefix_count) {
-            const long f = e->fs.match_key(m.packed);
-            if (f < 0) continue;
-            m.filter = (uint32_t)f;
-        }
-        if (k == cap)
-            return fail(err, errlen, OG_E_CAPACITY, "more than %zu matches and room for %zu in the caller's buffer",
-                        cap, cap);
-        m.offset = offset_of(h);
-        out[k++] = m;
-    }
+    const size_t k = confirm_matches(e, reinterpret_cast<MatchRec*>(e->h_recs.p), matched);
+    if (k > cap) return fail(err, errlen, OG_E_CAPACITY, "%zu matches and room for %zu in the caller's buffer", k, cap);
+    std::memcpy(out, stage, k * sizeof(og_match));
     *n = k;
+    return OG_OK;
+}
+
+int og_engine_collect_matches_view(og_engine* e, const og_match** matches, size_t* n, char* err, size_t errlen) {
+    if (!e || !matches || !n) return fail(err, errlen, OG_E_ARG, "null argument");
+    *matches = nullptr;
+    *n = 0;
+    uint32_t matched = 0;
+    uint64_t launch = 0;
+    const void* src = nullptr;
+    int rc = collect_flight(e, true, &matched, &launch, &src, err, errlen);
+    if (rc != OG_OK) return rc;
+    // nothing to convert: the calling thread only waits for the chunks
+    rc = copy_records(e, static_cast<const MatchRec*>(src), matched, [](size_t, size_t) {}, err, errlen, 1);
+    if (rc != OG_OK) return rc;
+    MatchRec* stage = reinterpret_cast<MatchRec*>(e->h_recs.p);
+    *n = e->long_filters ? confirm_matches(e, stage, matched) : matched;
+    *matches = reinterpret_cast<const og_match*>(stage);
     return OG_OK;
 }
 

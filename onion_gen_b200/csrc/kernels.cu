@@ -216,9 +216,13 @@ __global__ void __launch_bounds__(128) match_kernel(const MatchArgs a) {
         if (owner != 0xffffffffu) {
             const uint32_t idx = atomicAdd(a.out_count, 1u);
             if (idx < a.out_cap) {
-                HitRec h = r;
-                h.pad = owner;
-                a.out[idx] = h;
+                // window w = window0 + round * lanes + lane; candidate i of it
+                const uint64_t w = a.window0 + (uint64_t)(r.step / a.slots) * a.lanes + r.lane;
+                const uint64_t k = w * a.slots + (a.paired ? 1u : 0u) + r.step % a.slots;
+                uint4* dst = reinterpret_cast<uint4*>(a.out + idx);
+                dst[0] = make_uint4((uint32_t)(8 * k), (uint32_t)((8 * k) >> 32), r.y[0], r.y[1]);
+                dst[1] = make_uint4(r.y[2], r.y[3], r.y[4], r.y[5]);
+                dst[2] = make_uint4(r.y[6], r.y[7], owner, 0u);
             }
         }
     }

@@ -40,6 +40,18 @@ struct HitRec {
 };
 static_assert(sizeof(HitRec) == 48, "HitRec layout");
 
+// A device exact match in the caller's layout (og_match): the candidate's
+// scalar offset, its canonical y limbs (the packed key's little-endian
+// bytes) and the filter it matched. The match kernel decodes the offset, so
+// the host copies the records through unchanged.
+struct MatchRec {
+    uint64_t offset;
+    uint32_t y[8];
+    uint32_t filter;
+    uint32_t pad;
+};
+static_assert(sizeof(MatchRec) == 48, "MatchRec layout");
+
 struct FeWords {
     uint32_t v[8];
 };
@@ -148,7 +160,7 @@ struct MatchArgs {
     uint32_t lanes;
     uint32_t slots;
     uint32_t paired;           // offsets 8 (w slots + 1 + i), else 8 (w slots + i)
-    HitRec* out;
+    MatchRec* out;
     uint32_t* out_count;
     uint32_t out_cap;
     uint32_t* mismatch;        // survivors whose recomputed key differs from their record

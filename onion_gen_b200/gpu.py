@@ -205,8 +205,25 @@ class Engine:
         N.check(N.lib.og_engine_collect_matches(self._h, self._mbuf, self._room, C.byref(n), err, 512), err)
         return self._matches(n.value)
 
-    def _matches(self, k):
-        raw = np.frombuffer(self._mbuf, dtype=np.uint8, count=k * 48).reshape(k, 48)
+    def collect_matches_view(self):
+        """og_engine_collect_matches_view: the oldest launched advance's
+        matches where the engine keeps them (its pinned host memory), as a
+        ctypes array of ``Match`` valid until the next collect; no copy."""
+        p = C.c_void_p()
+        n = C.c_size_t()
+        err = N.errbuf()
+        N.check(N.lib.og_engine_collect_matches_view(self._h, C.byref(p), C.byref(n), err, 512), err)
+        if n.value == 0:
+            return (N.Match * 0)()
+        return (N.Match * n.value).from_address(p.value)
+
+    def collect_matches_view_raw(self):
+        """collect_matches_view copied out as (offsets, packed, filters) arrays."""
+        view = self.collect_matches_view()
+        return self._matches(len(view), view)
+
+    def _matches(self, k, buf=None):
+        raw = np.frombuffer(self._mbuf if buf is None else buf, dtype=np.uint8, count=k * 48).reshape(k, 48)
         offsets = raw[:, :8].copy().view(np.uint64).reshape(k)
         filters = raw[:, 40:44].copy().view(np.uint32).reshape(k)
         return offsets, raw[:, 8:40].copy(), filters

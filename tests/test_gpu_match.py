@@ -224,3 +224,61 @@ def test_chain_scheme_device_match_equals_host_match(device):
     for o, packed, f in got[:50]:
         pk, _ = key.check_hit(workloads.seed(4), o, packed)
         assert fs.match_address(pk) == f
+
+
+def view_matches(eng, advances):
+    out = []
+    for _ in range(advances):
+        eng.launch_matches()
+        o, k, f = eng.collect_matches_view_raw()
+        out.extend((int(a), bytes(b), int(c)) for a, b, c in zip(o, k, f))
+    return sorted(out)
+
+
+def test_matches_view_equals_host_match(device):
+    """og_engine_collect_matches_view leaves each advance's matches in the
+    engine's pinned memory in og_match's layout, their offsets decoded on the
+    device: they equal the host's match of the same engine's survivors,
+    filters longer than the device tables confirmed on the host included
+    (the decoy that shares 12 symbols is dropped). With two advances in
+    flight the views come back in launch order."""
+    seed = workloads.seed(0)
+    start = key.start_point(seed)
+    off = 8 * (5 * SLOTS + 1 + 17)
+    text = key.address(key_at(seed, off))
+    decoy = text[:12] + ("a" if text[12] != "a" else "b") + text[13]
+    fs = F.FilterSet.parse_all(workloads.config3_prefixes(2000) + [text[:14], decoy])
+    words, bits = fs.index_words()
+    plain = gpu.Engine(device, start, bitmap=words, bitmap_bits=bits, config=cfg())
+    want = host_matches(plain, fs, 3)
+    plain.close()
+    v = gpu.Engine(device, start, bitmap=words, bitmap_bits=bits, config=cfg())
+    v.match_on_device(fs)
+    got = view_matches(v, 3)
+    v.close()
+    assert len(want) > 1000 and got == want
+    assert [g for g in got if g[0] == off][0][2] == fs.texts().index(text[:14])
+    # two in flight: launch, launch, view, launch, view, view
+    w = gpu.Engine(device, start, bitmap=words, bitmap_bits=bits, config=cfg())
+    w.match_on_device(fs)
+    w.launch_matches()
+    w.launch_matches()
+    views = [w.collect_matches_view_raw()]
+    w.launch_matches()
+    views += [w.collect_matches_view_raw(), w.collect_matches_view_raw()]
+    w.close()
+    flat = sorted((int(a), bytes(b), int(c)) for o, k, f in views for a, b, c in zip(o, k, f))
+    assert flat == want
+    # each advance's matches lie in its own range of offsets, in launch order
+    tops = [int(o.max()) for o, _, _ in views]
+    bottoms = [int(o.min()) for o, _, _ in views]
+    assert tops[0] < bottoms[1] and tops[1] < bottoms[2]
+    with pytest.raises(N.OgError) as e:
+        w2 = gpu.Engine(device, start, bitmap=words, bitmap_bits=bits, config=cfg())
+        try:
+            w2.match_on_device(fs)
+            w2.launch()
+            w2.collect_matches_view()
+        finally:
+            w2.close()
+    assert e.value.status == "OG_E_STATE"

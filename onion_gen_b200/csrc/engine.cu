@@ -685,14 +685,14 @@ int copy_records(og_engine* e, const Rec* src, size_t n, F&& body, char* err, si
         if (ce == cudaSuccess) ce = cudaEventRecord(e->chunk_ev[c], e->cstream);
     }
     std::atomic<int> failed{(int)ce};
-    const auto work = [&](size_t t, size_t workers) {
+    const auto work = [&](size_t t, size_t nw) {
         for (size_t c = 0; c < chunks && failed.load() == cudaSuccess; c++) {
             const cudaError_t we = cudaEventSynchronize(e->chunk_ev[c]);
             if (we != cudaSuccess) {
                 failed.store((int)we);
                 return;
             }
-            const size_t lo = c * per, hi = std::min(n, lo + per), slice = (hi - lo + workers - 1) / workers;
+            const size_t lo = c * per, hi = std::min(n, lo + per), slice = (hi - lo + nw - 1) / nw;
             const size_t a = std::min(hi, lo + t * slice), b = std::min(hi, a + slice);
             if (a < b) body(a, b);
         }
